@@ -1,0 +1,213 @@
+/*
+ * nsat.h -- C ABI of the B200 exhaustive circuit solver (libnsat.so).
+ *
+ * The reference (matszpk/naivesat) plugs its solvers into the external
+ * gatenative crate: a builder compiles a Gate circuit plus a C/OpenCL
+ * "aggr_output" snippet into a bit-sliced kernel, and a mapper calls it once
+ * per value of the "arg" inputs (main.rs:106-264, qsat.rs:1599-1836,
+ * greedysatostop.rs:634-837, 1042-1099).  This ABI replaces that whole
+ * builder/mapper/snippet stack with one call per solve.  Every entry point
+ * returns an int status (0 = OK, negative = error, never aborts); a context is
+ * bound to one device and one stream and must not be used by two threads at
+ * once; separate contexts are independent.
+ *
+ * Circuit encoding: wires 0..n-1 are the inputs, wire n+k is gate k.
+ *   gates[3k] = function (NSAT_AND/NOR/NIMPL/XOR), gates[3k+1] = i0,
+ *   gates[3k+2] = i1 (< n+k);  outputs[2j] = wire, outputs[2j+1] = negated.
+ * This is the shape of gatesim's Circuit::new(n, gates, outputs) as used at
+ * qsat.rs:2630 and satostop.rs:1792.
+ */
+#ifndef NSAT_H
+#define NSAT_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NSAT_OK 0
+#define NSAT_EINVAL (-1)        /* bad argument or malformed circuit */
+#define NSAT_ENOMEM (-2)        /* host or device allocation failed */
+#define NSAT_ECOMPILE (-3)      /* NVRTC compile or module load failed */
+#define NSAT_ECUDA (-4)         /* a CUDA call failed */
+#define NSAT_ETIMEOUT (-5)      /* a bounded device wait ran out */
+#define NSAT_ENODEV (-6)        /* no usable CUDA device */
+#define NSAT_EUNSUPPORTED (-7)  /* size outside what this build handles */
+#define NSAT_EPARSE (-8)        /* circuit text could not be parsed */
+#define NSAT_EBUSY (-9)         /* admission refused (serving queue full) */
+
+enum { NSAT_AND = 0, NSAT_NOR = 1, NSAT_NIMPL = 2, NSAT_XOR = 3 };
+
+typedef struct nsat_ctx nsat_ctx;
+typedef struct nsat_circuit nsat_circuit;
+typedef struct nsat_table nsat_table;
+typedef struct nsat_parsed nsat_parsed;
+
+typedef struct {
+    uint32_t input_len;
+    uint32_t gate_num;
+    const uint32_t* gates;    /* 3 * gate_num */
+    uint32_t output_num;
+    const uint32_t* outputs;  /* 2 * output_num */
+} nsat_circuit_desc;
+
+typedef struct {
+    uint32_t block_threads;   /* CUDA block size; 0 = auto.  The reference's -G
+                                 (OpenCL group length, main.rs:70-73) maps here */
+    uint32_t no_optimize;     /* 1 = one logic op per gate, no LOP3 cut mapping.
+                                 The reference's -n (optimize_negs off) maps here */
+    uint32_t verbose;         /* 1 = print JIT/launch details on stderr */
+    uint32_t reserved;
+} nsat_opts;
+
+/* ---- context ------------------------------------------------------------ */
+/* Replaces OpenCLBuilder::new(&device, config) / CPUBuilder::new (main.rs:278-300). */
+int nsat_create(int device, const nsat_opts* opts, nsat_ctx** out);
+void nsat_destroy(nsat_ctx* ctx);
+const char* nsat_strerror(int status);
+/* Last error detail of this context (empty string if none). */
+const char* nsat_last_error(const nsat_ctx* ctx);
+/* Number of visible CUDA devices (0 when none); never fails. */
+int nsat_device_count(void);
+
+/* ---- circuits ----------------------------------------------------------- */
+/* Replaces builder.add_with_config(name, circuit, CodeConfig) (main.rs:113-123):
+ * validates and copies the circuit; kernels are generated and NVRTC-compiled
+ * lazily on first use per solve kind and cached by content hash. */
+int nsat_circuit_new(nsat_ctx* ctx, const nsat_circuit_desc* desc, nsat_circuit** out);
+void nsat_circuit_free(nsat_circuit* c);
+/* LUT statistics after cut mapping of output `output` (or all outputs when
+ * output < 0): live two-input gates and LOP3 operations emitted. */
+int nsat_circuit_stats(nsat_ctx* ctx, nsat_circuit* c, int output,
+                       uint32_t* live_gates, uint32_t* lop3_ops);
+
+/* Parses gatesim text: Circuit::from_str (main.rs:390) or, with a quantifier
+ * prefix, QuantCircuit::from_str (qsat.rs:6276-6285). */
+int nsat_parse(const char* text, size_t len, nsat_parsed** out);
+/* quants: NULL if the text had no quantifiers, else input_len bytes, 1 = All. */
+int nsat_parsed_get(const nsat_parsed* p, nsat_circuit_desc* desc, const uint8_t** quants);
+void nsat_parsed_free(nsat_parsed* p);
+/* Writes gatesim text; returns the needed size (without NUL) in *needed. */
+int nsat_format(const nsat_circuit_desc* desc, const uint8_t* quants, char* buf,
+                size_t buflen, size_t* needed);
+
+/* ---- SAT (naivesat) ----------------------------------------------------- */
+/* Replaces do_command_with_{par,opencl,parseq}_mapper with AGGR_OUTPUT_*_CODE
+ * (main.rs:76-264).  Natural order: input b is bit b of the assignment index.
+ * Output 0 of the circuit is the formula. */
+typedef struct {
+    uint32_t find_all;     /* 0: stop after the first chunk holding a solution and
+                              return the lowest one (naivesat); 1: scan the
+                              whole range, exact count and lowest witness */
+    uint32_t chunk_bits;   /* log2 assignments per launch (0 = auto).  The
+                              reference's -e elem_inputs maps here */
+    uint64_t begin_lo, begin_hi;  /* first index of the range (chunk aligned) */
+    uint64_t end_lo, end_hi;      /* end of range; both 0 = 2^n */
+} nsat_sat_opts;
+
+typedef struct {
+    int32_t satisfiable;
+    uint32_t launches;
+    uint64_t count_lo, count_hi;      /* solutions among the scanned indices */
+    uint64_t witness_lo, witness_hi;  /* lowest satisfying index */
+    uint64_t scanned_lo, scanned_hi;  /* assignments scanned */
+    double device_ms;                 /* kernel time, CUDA events */
+    double wall_ms;                   /* host time of the call */
+} nsat_sat_result;
+
+int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opts* opts,
+                   nsat_sat_result* res);
+
+/* ---- QSAT (naiveqsat) --------------------------------------------------- */
+/* Replaces MainOpenCLQuantReducer/OpenCLQuantReducer/QuantReducer and the
+ * QSAT aggr snippets (qsat.rs:172-1597).  v-order: input i is bit n-1-i of
+ * the item index, so input 0 is the outermost quantifier.  The answer equals
+ * pushing every circuit value in order into a QuantReducer (qsat.rs:1991). */
+typedef struct {
+    uint32_t chunk_bits;   /* log2 assignments per launch (0 = auto) */
+    uint32_t reserved;
+} nsat_qsat_opts;
+
+typedef struct {
+    int32_t reversed;          /* first quantifier is All */
+    uint32_t solution_bits;    /* length of the first quantifier block */
+    int32_t has_solution;
+    int32_t value;             /* truth value of the quantified formula */
+    uint64_t solution_lo, solution_hi;  /* bit k = input k of the first block */
+    uint32_t launches;
+    uint32_t reserved;
+    double device_ms;
+    double wall_ms;
+} nsat_qsat_result;
+
+int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
+                    const nsat_qsat_opts* opts, nsat_qsat_result* res);
+
+/* Runs the QSAT reduction kernel on raw item bits instead of a circuit
+ * (item k = bit k%32 of words[k/32], 2^nq items, nq >= 5): the analogue of
+ * the reference's identity-circuit aggregator tests (qsat.rs:2629-3520). */
+int nsat_qsat_reduce_words(nsat_ctx* ctx, const uint8_t* quants, uint32_t nq,
+                           const uint32_t* words, nsat_qsat_result* res);
+
+/* ---- SATOSTOP (greedysatostop, naivesatostop) ---------------------------- */
+/* Replaces the greedy OpenCL table aggr + join_nexts/check_stop/find_solution
+ * kernels (greedysatostop.rs:841-1099).  The circuit has n inputs and n+1
+ * outputs: outputs 0..n-1 are the next state, output n is STOP. */
+typedef struct {
+    uint32_t want_steps;   /* carry evaluation counts (naivesatostop's steps) */
+    uint32_t reserved;
+} nsat_table_opts;
+
+int nsat_stop_table_build(nsat_ctx* ctx, nsat_circuit* c, const nsat_table_opts* opts,
+                          nsat_table** out);
+void nsat_table_free(nsat_table* t);
+/* Copies entries [first, first+count) as next | STOP << n (device -> host). */
+int nsat_table_read(nsat_table* t, uint64_t first, uint64_t count, uint64_t* out);
+/* Bytes of device memory held by the table (both ping-pong buffers). */
+uint64_t nsat_table_bytes(const nsat_table* t);
+
+typedef struct {
+    uint32_t unknowns;     /* the top `unknowns` state bits are the unknowns */
+    uint32_t mode;         /* 0: lowest start among those resolved in the first
+                              doubling round that resolves any (greedy loop,
+                              greedysatostop.rs:1084-1091); 1: lowest start
+                              that stops at all (naivesatostop -S order) */
+} nsat_stop_opts;
+
+typedef struct {
+    int32_t found;
+    uint32_t rounds;       /* doubling rounds run */
+    uint64_t start, end, steps;   /* steps only with want_steps */
+    double build_ms, join_ms;
+} nsat_stop_result;
+
+int nsat_stop_solve(nsat_ctx* ctx, nsat_table* t, const nsat_stop_opts* opts,
+                    nsat_stop_result* res);
+
+/* ---- build check -------------------------------------------------------- */
+/* Generates and NVRTC-compiles for sm_100a, without a device, the kernel that
+ * a solve of `kind` (0 = SAT, 1 = QSAT, 2 = SATOSTOP table) would launch for
+ * this circuit, and reports ptxas resource usage.  Plays the role of the
+ * reference's mapper.build() step (main.rs:124), minus the device.
+ * quants is required for kind 1.  log (may be NULL) receives the compile log. */
+typedef struct {
+    int32_t regs;           /* registers per thread */
+    int32_t spill_bytes;    /* spill stores per thread */
+    uint32_t lop3_ops;      /* LOP3 operations per 32-lane word */
+    uint32_t live_gates;    /* two-input gates in the output cone */
+    double compile_ms;
+} nsat_jit_info;
+
+int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quants, int kind,
+                   const nsat_opts* opts, nsat_jit_info* info, char* log, size_t loglen);
+
+/* ---- measurement -------------------------------------------------------- */
+/* Measures this device's 32-bit LOP3 issue rate with a chain microbenchmark
+ * (independent lop3.b32 chains, no memory traffic): thread-instructions/s. */
+int nsat_probe_lop3_peak(nsat_ctx* ctx, double* lop3_per_s, double* sm_clock_mhz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,355 @@
+"""ctypes binding of libnsat.so (the C ABI in include/nsat.h).
+
+This is the Python face of the same entry points the command-line tools use.
+There is no fallback: if libnsat.so is missing or no CUDA device is present,
+the calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnsat.so")
+
+NSAT_OK = 0
+ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECOMPILE", -4: "ECUDA", -5: "ETIMEOUT", -6: "ENODEV",
+          -7: "EUNSUPPORTED", -8: "EPARSE", -9: "EBUSY"}
+
+U8P = C.POINTER(C.c_uint8)
+U32P = C.POINTER(C.c_uint32)
+U64P = C.POINTER(C.c_uint64)
+
+
+class CircuitDesc(C.Structure):
+    _fields_ = [("input_len", C.c_uint32), ("gate_num", C.c_uint32), ("gates", U32P),
+                ("output_num", C.c_uint32), ("outputs", U32P)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("no_optimize", C.c_uint32),
+                ("verbose", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class SatOpts(C.Structure):
+    _fields_ = [("find_all", C.c_uint32), ("chunk_bits", C.c_uint32),
+                ("begin_lo", C.c_uint64), ("begin_hi", C.c_uint64),
+                ("end_lo", C.c_uint64), ("end_hi", C.c_uint64)]
+
+
+class SatResult(C.Structure):
+    _fields_ = [("satisfiable", C.c_int32), ("launches", C.c_uint32),
+                ("count_lo", C.c_uint64), ("count_hi", C.c_uint64),
+                ("witness_lo", C.c_uint64), ("witness_hi", C.c_uint64),
+                ("scanned_lo", C.c_uint64), ("scanned_hi", C.c_uint64),
+                ("device_ms", C.c_double), ("wall_ms", C.c_double)]
+
+
+class QsatOpts(C.Structure):
+    _fields_ = [("chunk_bits", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class QsatResult(C.Structure):
+    _fields_ = [("reversed", C.c_int32), ("solution_bits", C.c_uint32),
+                ("has_solution", C.c_int32), ("value", C.c_int32),
+                ("solution_lo", C.c_uint64), ("solution_hi", C.c_uint64),
+                ("launches", C.c_uint32), ("reserved", C.c_uint32),
+                ("device_ms", C.c_double), ("wall_ms", C.c_double)]
+
+
+class JitInfo(C.Structure):
+    _fields_ = [("regs", C.c_int32), ("spill_bytes", C.c_int32), ("lop3_ops", C.c_uint32),
+                ("live_gates", C.c_uint32), ("compile_ms", C.c_double)]
+
+
+class TableOpts(C.Structure):
+    _fields_ = [("want_steps", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class StopOpts(C.Structure):
+    _fields_ = [("unknowns", C.c_uint32), ("mode", C.c_uint32)]
+
+
+class StopResult(C.Structure):
+    _fields_ = [("found", C.c_int32), ("rounds", C.c_uint32), ("start", C.c_uint64),
+                ("end", C.c_uint64), ("steps", C.c_uint64), ("build_ms", C.c_double),
+                ("join_ms", C.c_double)]
+
+
+EXPORTS = [
+    "nsat_create", "nsat_destroy", "nsat_strerror", "nsat_last_error", "nsat_device_count",
+    "nsat_circuit_new", "nsat_circuit_free", "nsat_circuit_stats", "nsat_parse",
+    "nsat_parsed_get", "nsat_parsed_free", "nsat_format", "nsat_sat_solve", "nsat_qsat_solve",
+    "nsat_qsat_reduce_words", "nsat_stop_table_build", "nsat_table_free", "nsat_table_read",
+    "nsat_table_bytes", "nsat_stop_solve", "nsat_probe_lop3_peak", "nsat_jit_check",
+]
+
+_lib = None
+
+
+def lib():
+    """Loads libnsat.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libnsat.so is not built: run `make -C naivesat_b200/csrc` "
+                               "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        L.nsat_create.argtypes = [C.c_int, C.POINTER(Opts), C.POINTER(C.c_void_p)]
+        L.nsat_destroy.argtypes = [C.c_void_p]
+        L.nsat_destroy.restype = None
+        L.nsat_strerror.argtypes = [C.c_int]
+        L.nsat_strerror.restype = C.c_char_p
+        L.nsat_last_error.argtypes = [C.c_void_p]
+        L.nsat_last_error.restype = C.c_char_p
+        L.nsat_device_count.argtypes = []
+        L.nsat_circuit_new.argtypes = [C.c_void_p, C.POINTER(CircuitDesc), C.POINTER(C.c_void_p)]
+        L.nsat_circuit_free.argtypes = [C.c_void_p]
+        L.nsat_circuit_free.restype = None
+        L.nsat_circuit_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_int, U32P, U32P]
+        L.nsat_parse.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p)]
+        L.nsat_parsed_get.argtypes = [C.c_void_p, C.POINTER(CircuitDesc), C.POINTER(U8P)]
+        L.nsat_parsed_free.argtypes = [C.c_void_p]
+        L.nsat_parsed_free.restype = None
+        L.nsat_format.argtypes = [C.POINTER(CircuitDesc), U8P, C.c_char_p, C.c_size_t,
+                                  C.POINTER(C.c_size_t)]
+        L.nsat_sat_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(SatOpts), C.POINTER(SatResult)]
+        L.nsat_qsat_solve.argtypes = [C.c_void_p, C.c_void_p, U8P, C.POINTER(QsatOpts),
+                                      C.POINTER(QsatResult)]
+        L.nsat_qsat_reduce_words.argtypes = [C.c_void_p, U8P, C.c_uint32, U32P, C.POINTER(QsatResult)]
+        L.nsat_stop_table_build.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(TableOpts),
+                                            C.POINTER(C.c_void_p)]
+        L.nsat_table_free.argtypes = [C.c_void_p]
+        L.nsat_table_free.restype = None
+        L.nsat_table_read.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, U64P]
+        L.nsat_table_bytes.argtypes = [C.c_void_p]
+        L.nsat_table_bytes.restype = C.c_uint64
+        L.nsat_stop_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(StopOpts), C.POINTER(StopResult)]
+        L.nsat_probe_lop3_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.nsat_jit_check.argtypes = [C.POINTER(CircuitDesc), U8P, C.c_int, C.POINTER(Opts),
+                                     C.POINTER(JitInfo), C.c_char_p, C.c_size_t]
+        _lib = L
+    return _lib
+
+
+class NsatError(RuntimeError):
+    pass
+
+
+def _quants_array(quants, n):
+    if isinstance(quants, str):
+        q = np.array([1 if ch in "Aa" else 0 for ch in quants], dtype=np.uint8)
+    else:
+        q = np.ascontiguousarray(np.asarray(quants, dtype=np.uint8))
+    if len(q) != n:
+        raise ValueError("need one quantifier per input")
+    return q
+
+
+def desc_of(n, gates, outputs):
+    g = np.ascontiguousarray(np.asarray(gates, dtype=np.uint32).reshape(-1))
+    o = np.ascontiguousarray(np.asarray(outputs, dtype=np.uint32).reshape(-1))
+    d = CircuitDesc(int(n), len(g) // 3, g.ctypes.data_as(U32P), len(o) // 2, o.ctypes.data_as(U32P))
+    d._keep = (g, o)
+    return d
+
+
+class Context:
+    """One device + stream; not for concurrent use from several threads."""
+
+    def __init__(self, device=0, block_threads=0, no_optimize=False, verbose=False):
+        L = lib()
+        h = C.c_void_p()
+        o = Opts(block_threads, 1 if no_optimize else 0, 1 if verbose else 0, 0)
+        rc = L.nsat_create(device, C.byref(o), C.byref(h))
+        if rc != NSAT_OK:
+            raise NsatError("nsat_create(%d): %s" % (device, L.nsat_strerror(rc).decode()))
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc != NSAT_OK:
+            msg = lib().nsat_last_error(self.h).decode(errors="replace")
+            raise NsatError("%s: %s (%s) %s" % (what, ERRORS.get(rc, rc), lib().nsat_strerror(rc).decode(), msg))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nsat_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def circuit(self, circ):
+        """Loads a workloads.Circuit (or anything with n, gates, outputs)."""
+        return CircuitHandle(self, circ.n, circ.gates, circ.outputs)
+
+    def lop3_peak(self):
+        r, mhz = C.c_double(), C.c_double()
+        self._check(lib().nsat_probe_lop3_peak(self.h, C.byref(r), C.byref(mhz)), "probe")
+        return r.value, mhz.value
+
+    def qsat_reduce_words(self, quants, words):
+        q = _quants_array(quants, len(quants))
+        w = np.ascontiguousarray(np.asarray(words, dtype=np.uint32))
+        assert len(w) * 32 == 1 << len(q)
+        r = QsatResult()
+        self._check(lib().nsat_qsat_reduce_words(self.h, q.ctypes.data_as(U8P), len(q),
+                                                 w.ctypes.data_as(U32P), C.byref(r)), "reduce_words")
+        return _qsat_dict(r)
+
+
+def _qsat_dict(r):
+    return {"reversed": bool(r.reversed), "solution_bits": r.solution_bits,
+            "solution": (r.solution_lo | (r.solution_hi << 64)) if r.has_solution else None,
+            "value": bool(r.value), "launches": r.launches, "device_ms": r.device_ms,
+            "wall_ms": r.wall_ms}
+
+
+class CircuitHandle:
+    def __init__(self, ctx, n, gates, outputs):
+        self.ctx = ctx
+        self.n = int(n)
+        d = desc_of(n, gates, outputs)
+        h = C.c_void_p()
+        ctx._check(lib().nsat_circuit_new(ctx.h, C.byref(d), C.byref(h)), "circuit_new")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().nsat_circuit_free(self.h)
+            self.h = None
+
+    def stats(self, output=0):
+        live, ops = C.c_uint32(), C.c_uint32()
+        self.ctx._check(lib().nsat_circuit_stats(self.ctx.h, self.h, output, C.byref(live),
+                                                 C.byref(ops)), "stats")
+        return live.value, ops.value
+
+    def sat(self, find_all=True, chunk_bits=0, begin=0, end=0):
+        o = SatOpts(1 if find_all else 0, chunk_bits, begin & 0xFFFFFFFFFFFFFFFF, begin >> 64,
+                    end & 0xFFFFFFFFFFFFFFFF, end >> 64)
+        r = SatResult()
+        self.ctx._check(lib().nsat_sat_solve(self.ctx.h, self.h, C.byref(o), C.byref(r)), "sat_solve")
+        return {"satisfiable": bool(r.satisfiable), "count": r.count_lo | (r.count_hi << 64),
+                "witness": (r.witness_lo | (r.witness_hi << 64)) if r.satisfiable else None,
+                "scanned": r.scanned_lo | (r.scanned_hi << 64), "launches": r.launches,
+                "device_ms": r.device_ms, "wall_ms": r.wall_ms}
+
+    def qsat(self, quants, chunk_bits=0):
+        q = _quants_array(quants, self.n)
+        o = QsatOpts(chunk_bits, 0)
+        r = QsatResult()
+        self.ctx._check(lib().nsat_qsat_solve(self.ctx.h, self.h, q.ctypes.data_as(U8P), C.byref(o),
+                                              C.byref(r)), "qsat_solve")
+        return _qsat_dict(r)
+
+    def stop_table(self, want_steps=False):
+        return Table(self, want_steps)
+
+
+class Table:
+    def __init__(self, circ, want_steps=False):
+        self.ctx = circ.ctx
+        self.n = circ.n
+        h = C.c_void_p()
+        o = TableOpts(1 if want_steps else 0, 0)
+        self.ctx._check(lib().nsat_stop_table_build(self.ctx.h, circ.h, C.byref(o), C.byref(h)),
+                        "stop_table_build")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().nsat_table_free(self.h)
+            self.h = None
+
+    def read(self, first=0, count=None):
+        if count is None:
+            count = (1 << self.n) - first
+        out = np.zeros(count, dtype=np.uint64)
+        self.ctx._check(lib().nsat_table_read(self.h, first, count, out.ctypes.data_as(U64P)), "table_read")
+        return out
+
+    def nbytes(self):
+        return lib().nsat_table_bytes(self.h)
+
+    def solve(self, unknowns, mode=0):
+        o = StopOpts(unknowns, mode)
+        r = StopResult()
+        self.ctx._check(lib().nsat_stop_solve(self.ctx.h, self.h, C.byref(o), C.byref(r)), "stop_solve")
+        if not r.found:
+            return {"found": False, "rounds": r.rounds, "build_ms": r.build_ms, "join_ms": r.join_ms}
+        return {"found": True, "start": r.start, "end": r.end, "steps": r.steps, "rounds": r.rounds,
+                "build_ms": r.build_ms, "join_ms": r.join_ms}
+
+
+def parse(text):
+    """gatesim text -> (n, gates (g,3), outputs (o,2), quants string or None)."""
+    L = lib()
+    b = text.encode()
+    h = C.c_void_p()
+    rc = L.nsat_parse(b, len(b), C.byref(h))
+    if rc != NSAT_OK:
+        raise NsatError("parse: %s" % ERRORS.get(rc, rc))
+    try:
+        d = CircuitDesc()
+        q = U8P()
+        L.nsat_parsed_get(h, C.byref(d), C.byref(q))
+        gates = np.ctypeslib.as_array(d.gates, (d.gate_num * 3,)).reshape(-1, 3).copy() if d.gate_num else \
+            np.zeros((0, 3), dtype=np.uint32)
+        outs = np.ctypeslib.as_array(d.outputs, (d.output_num * 2,)).reshape(-1, 2).copy()
+        quants = None
+        if q:
+            quants = "".join("A" if q[i] else "E" for i in range(d.input_len))
+        return d.input_len, gates, outs, quants
+    finally:
+        L.nsat_parsed_free(h)
+
+
+def format_circuit(n, gates, outputs, quants=None):
+    L = lib()
+    d = desc_of(n, gates, outputs)
+    qa = _quants_array(quants, n) if quants is not None else None
+    need = C.c_size_t()
+    qp = qa.ctypes.data_as(U8P) if qa is not None else None
+    rc = L.nsat_format(C.byref(d), qp, None, 0, C.byref(need))
+    if rc != NSAT_OK:
+        raise NsatError("format: %s" % ERRORS.get(rc, rc))
+    buf = C.create_string_buffer(need.value + 1)
+    rc = L.nsat_format(C.byref(d), qp, buf, need.value + 1, C.byref(need))
+    if rc != NSAT_OK:
+        raise NsatError("format: %s" % ERRORS.get(rc, rc))
+    return buf.value.decode()
+
+
+KIND = {"sat": 0, "qsat": 1, "table": 2}
+
+
+def jit_check(circ, kind="sat", quants=None, block_threads=0, no_optimize=False):
+    """NVRTC-compiles (no device needed) the kernel a solve would use; returns
+    ptxas resource usage and LUT statistics."""
+    L = lib()
+    d = desc_of(circ.n, circ.gates, circ.outputs)
+    q = _quants_array(quants, circ.n) if quants is not None else None
+    o = Opts(block_threads, 1 if no_optimize else 0, 0, 0)
+    info = JitInfo()
+    buf = C.create_string_buffer(1 << 16)
+    rc = L.nsat_jit_check(C.byref(d), q.ctypes.data_as(U8P) if q is not None else None, KIND[kind],
+                          C.byref(o), C.byref(info), buf, len(buf))
+    if rc != NSAT_OK:
+        raise NsatError("jit_check: %s\n%s" % (ERRORS.get(rc, rc), buf.value.decode(errors="replace")))
+    return {"regs": info.regs, "spill_bytes": info.spill_bytes, "lop3_ops": info.lop3_ops,
+            "live_gates": info.live_gates, "compile_ms": info.compile_ms,
+            "log": buf.value.decode(errors="replace")}
+
+
+def device_count():
+    return lib().nsat_device_count()

@@ -1,0 +1,917 @@
+// nsat_api.cpp -- the C ABI (include/nsat.h): contexts, circuits, and the SAT,
+// QSAT and SATOSTOP drivers around the NVRTC-specialised sm_100a kernels.
+#include "nsat.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "circuit.h"
+#include "codegen.h"
+#include "jit.h"
+#include "lutmap.h"
+#include "qreducer.h"
+#include "static_kernels.h"
+
+using namespace nsat;
+typedef unsigned __int128 u128;
+
+namespace {
+
+// Must match struct LaunchOut in device_template.cuh.
+struct LaunchOut {
+    uint64_t min_idx;
+    uint64_t count;
+    uint32_t tree;
+    uint32_t ticket;
+    uint32_t any;
+    uint32_t err;
+};
+static_assert(sizeof(LaunchOut) == 32, "LaunchOut layout");
+
+constexpr int kRing = 4;   // launches in flight before the host reads results
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+struct nsat_ctx {
+    int device = 0;
+    nsat_opts opts{};
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    std::string last_err;
+    LaunchOut* d_out = nullptr;       // kRing slots
+    LaunchOut* h_out = nullptr;       // pinned mirror
+    LaunchOut* h_init = nullptr;      // pinned init template
+    cudaEvent_t ev0[kRing]{}, ev1[kRing]{}, evd[kRing]{};
+    unsigned char* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    uint32_t* d_data = nullptr;
+    size_t data_bytes = 0;
+    NsatJoinState* d_join = nullptr;
+    NsatJoinState* h_join = nullptr;
+};
+
+struct nsat_circuit {
+    nsat_ctx* ctx = nullptr;
+    Circuit circ;
+    std::map<std::string, LutNet> nets;
+};
+
+struct nsat_table {
+    nsat_ctx* ctx = nullptr;
+    uint32_t n = 0, fmt = 0;
+    uint64_t N = 0;
+    size_t entry_bytes = 0;
+    void* buf[2] = {nullptr, nullptr};
+    int cur = 0;          // buffer holding the current table
+    bool any_stop = false;
+    double build_ms = 0;
+    ~nsat_table() {
+        if (buf[0] || buf[1]) {
+            cudaSetDevice(ctx->device);
+            if (buf[0]) cudaFree(buf[0]);
+            if (buf[1]) cudaFree(buf[1]);
+        }
+    }
+};
+
+struct nsat_parsed {
+    Parsed p;
+    std::vector<uint32_t> gates, outputs;
+};
+
+namespace {
+
+int fail(nsat_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->last_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? NSAT_ENOMEM : NSAT_ECUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    } while (0)
+
+int set_device(nsat_ctx* ctx) {
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return fail(ctx, NSAT_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return NSAT_OK;
+}
+
+Circuit from_desc(const nsat_circuit_desc* d) {
+    Circuit c;
+    c.n = d->input_len;
+    c.gates.resize(d->gate_num);
+    for (uint32_t k = 0; k < d->gate_num; k++)
+        c.gates[k] = Gate{(uint8_t)d->gates[3 * k], d->gates[3 * k + 1], d->gates[3 * k + 2]};
+    c.outputs.resize(d->output_num);
+    for (uint32_t j = 0; j < d->output_num; j++)
+        c.outputs[j] = Output{d->outputs[2 * j], d->outputs[2 * j + 1] != 0};
+    return c;
+}
+
+const LutNet& get_net(nsat_circuit* c, const std::vector<uint32_t>& which) {
+    std::string key = c->ctx->opts.no_optimize ? "raw:" : "lut:";
+    for (uint32_t j : which) key += std::to_string(j) + ",";
+    auto it = c->nets.find(key);
+    if (it != c->nets.end()) return it->second;
+    return c->nets[key] = map_luts(c->circ, which, c->ctx->opts.no_optimize != 0);
+}
+
+// Splits the launch's C enumeration bits into lane(5)+warp-lane(5)+IT+WB+CB.
+void choose_shape(uint32_t C, uint32_t block_threads, KernelConfig* kc) {
+    uint32_t wb = 3;
+    if (block_threads) {
+        wb = 0;
+        while ((32u << (wb + 1)) <= block_threads && wb < 5) wb++;
+    }
+    if (wb > C - 10) wb = C - 10;
+    uint32_t rest = C - 10 - wb;
+    uint32_t cb = std::min<uint32_t>(rest, 12);
+    uint32_t it = rest - cb;
+    if (it > 10) { it = 10; cb = rest - 10; }
+    kc->wb = wb; kc->it = it; kc->cb = cb; kc->c = C;
+}
+
+int ensure_scratch(nsat_ctx* ctx, size_t bytes) {
+    if (ctx->scratch_bytes >= bytes) return NSAT_OK;
+    if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+    ctx->d_scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    CK(cudaMalloc(&ctx->d_scratch, bytes));
+    ctx->scratch_bytes = bytes;
+    return NSAT_OK;
+}
+
+int get_kernel(nsat_ctx* ctx, const KernelConfig& kc, const LutNet& net, const char* name,
+               CUfunction* fn, std::shared_ptr<JitModule>* holder) {
+    std::string src = generate_source(kc, net);
+    std::string err;
+    int rc = jit_get(ctx->device, src, {name}, ctx->opts.verbose != 0, holder, &err);
+    if (rc == -3) return fail(ctx, NSAT_ECOMPILE, err);
+    if (rc != 0) return fail(ctx, NSAT_ECUDA, err);
+    *fn = (*holder)->fns[name];
+    return NSAT_OK;
+}
+
+int launch(nsat_ctx* ctx, CUfunction fn, unsigned grid, unsigned threads, void** params) {
+    std::string err;
+    const DriverApi* api = driver_api(&err);
+    if (!api) return fail(ctx, NSAT_ECUDA, err);
+    CUresult r = api->LaunchKernel(fn, grid, 1, 1, threads, 1, 1, 0, (CUstream)ctx->stream, params, nullptr);
+    if (r != CUDA_SUCCESS) {
+        const char* s = nullptr;
+        api->GetErrorString(r, &s);
+        return fail(ctx, NSAT_ECUDA, std::string("cuLaunchKernel: ") + (s ? s : "?"));
+    }
+    return NSAT_OK;
+}
+
+int ctz128(u128 v) {
+    if (v == 0) return 128;
+    uint64_t lo = (uint64_t)v;
+    if (lo) return __builtin_ctzll(lo);
+    return 64 + __builtin_ctzll((uint64_t)(v >> 64));
+}
+
+uint64_t reverse_bits(uint64_t v, uint32_t bits) {
+    uint64_t r = 0;
+    for (uint32_t k = 0; k < bits; k++) r |= ((v >> k) & 1ull) << (bits - 1 - k);
+    return r;
+}
+
+// Runs a sequence of launches of one kernel with a ring of result slots:
+// `issue(k, slot)` enqueues launch k, `consume(k, out, ms)` sees its result and
+// returns false to stop issuing.  Device time is the sum of the per-launch
+// CUDA event intervals.
+template <typename Issue, typename Consume>
+int run_ring(nsat_ctx* ctx, uint64_t total, Issue issue, Consume consume, double* dev_ms,
+             uint32_t* launches) {
+    uint64_t issued = 0, done = 0;
+    bool stop = false;
+    *dev_ms = 0;
+    *launches = 0;
+    while (done < issued || (!stop && issued < total)) {
+        if (!stop && issued < total && issued - done < (uint64_t)kRing) {
+            const int slot = (int)(issued % kRing);
+            CK(cudaMemcpyAsync(ctx->d_out + slot, ctx->h_init, sizeof(LaunchOut), cudaMemcpyHostToDevice,
+                               ctx->stream));
+            CK(cudaEventRecord(ctx->ev0[slot], ctx->stream));
+            int rc = issue(issued, slot);
+            if (rc) return rc;
+            CK(cudaEventRecord(ctx->ev1[slot], ctx->stream));
+            CK(cudaMemcpyAsync(ctx->h_out + slot, ctx->d_out + slot, sizeof(LaunchOut), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            CK(cudaEventRecord(ctx->evd[slot], ctx->stream));
+            issued++;
+            continue;
+        }
+        const int slot = (int)(done % kRing);
+        CK(cudaEventSynchronize(ctx->evd[slot]));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0[slot], ctx->ev1[slot]));
+        *dev_ms += ms;
+        (*launches)++;
+        if (!stop) {
+            if (!consume(done, ctx->h_out[slot])) stop = true;
+        }
+        done++;
+    }
+    return NSAT_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// kernel plans (shared by the solvers and nsat_jit_check)
+
+struct SatPlan {
+    KernelConfig kc;
+    uint32_t d = 0, C = 0;
+    u128 bp = 0, ep = 0;   // range in the padded index space
+};
+
+int plan_sat(uint32_t n, const nsat_sat_opts& o, uint32_t block_threads, SatPlan* pl, std::string* err) {
+    const uint32_t d = n < 15 ? 15 - n : 0;     // dummy low bits for tiny circuits
+    const uint32_t np = n + d;
+    if (np > 128) { *err = "too many inputs"; return NSAT_EUNSUPPORTED; }
+    const u128 full = (u128)1 << n;
+    u128 begin = ((u128)o.begin_hi << 64) | o.begin_lo;
+    u128 end = ((u128)o.end_hi << 64) | o.end_lo;
+    if (end == 0) end = full;
+    if (begin >= end || end > full) { *err = "bad range"; return NSAT_EINVAL; }
+    const u128 bp = begin << d, ep = end << d;
+    uint32_t C = o.chunk_bits ? std::max<uint32_t>(15, o.chunk_bits + d) : 34;
+    C = std::min<uint32_t>(C, np);
+    C = std::min<uint32_t>(C, (uint32_t)ctz128(bp));
+    C = std::min<uint32_t>(C, (uint32_t)ctz128(ep - bp));
+    if (C < 10) { *err = "range must be aligned to 2^10 assignments"; return NSAT_EINVAL; }
+    if (np - C > 64) { *err = "more than 2^64 launches"; return NSAT_EUNSUPPORTED; }
+    KernelConfig& kc = pl->kc;
+    kc.mode = Mode::SAT;
+    kc.nin = np;
+    kc.nb = np;
+    kc.in_of_bit.resize(np);
+    for (uint32_t p = 0; p < np; p++) kc.in_of_bit[p] = p < d ? -1 : (int)(p - d);
+    choose_shape(C, block_threads, &kc);
+    pl->d = d; pl->C = C; pl->bp = bp; pl->ep = ep;
+    return NSAT_OK;
+}
+
+struct QsatPlan {
+    KernelConfig kc;
+    std::vector<uint8_t> q;   // padded quantifiers
+    uint32_t n = 0, d = 0, np = 0, f = 0, m = 0, C = 0, A = 0;
+};
+
+int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint32_t chunk_bits,
+              uint32_t block_threads, QsatPlan* pl, std::string* err) {
+    if (quants_in.size() != n || n == 0) { *err = "quantifier count differs from inputs"; return NSAT_EINVAL; }
+    const uint32_t d = n < 15 ? 15 - n : 0;
+    const uint32_t np = n + d;
+    if (np > 128) { *err = "too many inputs"; return NSAT_EUNSUPPORTED; }
+    std::vector<uint8_t> q = quants_in;
+    for (uint32_t k = 0; k < d; k++) q.push_back(quants_in[n - 1] ? 0 : 1);
+    uint32_t f = 0;
+    while (f < n && q[f] == q[0]) f++;
+    const uint32_t m = np - f;
+    uint32_t C = chunk_bits ? std::max<uint32_t>(15, chunk_bits + d) : 34;
+    C = std::min<uint32_t>(C, np);
+    const uint32_t A = np - C;
+    if (A > 64) { *err = "more than 64 quantifiers above one launch"; return NSAT_EUNSUPPORTED; }
+    KernelConfig& kc = pl->kc;
+    kc.mode = Mode::QSAT;
+    kc.data = data;
+    kc.nin = np;
+    kc.nb = np;
+    kc.in_of_bit.resize(np);
+    for (uint32_t p = 0; p < np; p++) {
+        int in = (int)(np - 1 - p);
+        kc.in_of_bit[p] = (data || in >= (int)n) ? -1 : in;
+    }
+    choose_shape(C, block_threads, &kc);
+    kc.m = std::min<uint32_t>(m, 127);
+    kc.q0all = q[0] != 0;
+    kc.allbits = 0;
+    for (uint32_t j = 0; j < std::min<uint32_t>(C, 64); j++)
+        if (q[np - 1 - j]) kc.allbits |= 1ull << j;
+    pl->q = q; pl->n = n; pl->d = d; pl->np = np; pl->f = f; pl->m = m; pl->C = C; pl->A = A;
+    return NSAT_OK;
+}
+
+int plan_table(const Circuit& circ, bool steps, KernelConfig* kc, std::string* err) {
+    const uint32_t n = circ.n;
+    if (circ.outputs.size() != n + 1) { *err = "SATOSTOP circuit needs n+1 outputs"; return NSAT_EINVAL; }
+    if (n > 36) { *err = "state longer than 36 bits does not fit device memory"; return NSAT_EUNSUPPORTED; }
+    uint32_t fmt;
+    if (steps) {
+        if (n > 31) { *err = "steps need n <= 31"; return NSAT_EUNSUPPORTED; }
+        fmt = 2;
+    } else {
+        fmt = n <= 31 ? 0 : 1;
+    }
+    kc->mode = Mode::TABLE;
+    kc->nin = n;
+    kc->nb = n;
+    kc->in_of_bit.resize(n);
+    for (uint32_t p = 0; p < n; p++) kc->in_of_bit[p] = (int)p;
+    kc->wb = 3;
+    kc->fmt = fmt;
+    kc->nout = n + 1;
+    return NSAT_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// context
+
+extern "C" int nsat_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n;
+}
+
+extern "C" const char* nsat_strerror(int s) {
+    switch (s) {
+    case NSAT_OK: return "ok";
+    case NSAT_EINVAL: return "invalid argument";
+    case NSAT_ENOMEM: return "out of memory";
+    case NSAT_ECOMPILE: return "kernel compile failed";
+    case NSAT_ECUDA: return "CUDA error";
+    case NSAT_ETIMEOUT: return "device wait timed out";
+    case NSAT_ENODEV: return "no CUDA device";
+    case NSAT_EUNSUPPORTED: return "unsupported size";
+    case NSAT_EPARSE: return "parse error";
+    case NSAT_EBUSY: return "busy";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char* nsat_last_error(const nsat_ctx* ctx) { return ctx ? ctx->last_err.c_str() : ""; }
+
+extern "C" int nsat_create(int device, const nsat_opts* opts, nsat_ctx** out) {
+    if (!out) return NSAT_EINVAL;
+    *out = nullptr;
+    int ndev = nsat_device_count();
+    if (ndev <= 0) return NSAT_ENODEV;
+    if (device < 0 || device >= ndev) return NSAT_EINVAL;
+    std::unique_ptr<nsat_ctx> c(new nsat_ctx());
+    nsat_ctx* ctx = c.get();
+    ctx->device = device;
+    if (opts) ctx->opts = *opts;
+    if (set_device(ctx)) return NSAT_ECUDA;
+    CK(cudaFree(nullptr));
+    CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&ctx->d_out, sizeof(LaunchOut) * kRing));
+    CK(cudaMallocHost(&ctx->h_out, sizeof(LaunchOut) * kRing));
+    CK(cudaMallocHost(&ctx->h_init, sizeof(LaunchOut)));
+    CK(cudaMalloc(&ctx->d_join, sizeof(NsatJoinState)));
+    CK(cudaMallocHost(&ctx->h_join, sizeof(NsatJoinState)));
+    memset(ctx->h_init, 0, sizeof(LaunchOut));
+    ctx->h_init->min_idx = ~0ull;
+    for (int i = 0; i < kRing; i++) {
+        CK(cudaEventCreate(&ctx->ev0[i]));
+        CK(cudaEventCreate(&ctx->ev1[i]));
+        CK(cudaEventCreateWithFlags(&ctx->evd[i], cudaEventDisableTiming));
+    }
+    std::string err;
+    if (!driver_api(&err)) return NSAT_ECUDA;
+    *out = c.release();
+    return NSAT_OK;
+}
+
+extern "C" void nsat_destroy(nsat_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < kRing; i++) {
+        if (ctx->ev0[i]) cudaEventDestroy(ctx->ev0[i]);
+        if (ctx->ev1[i]) cudaEventDestroy(ctx->ev1[i]);
+        if (ctx->evd[i]) cudaEventDestroy(ctx->evd[i]);
+    }
+    cudaFree(ctx->d_out);
+    cudaFreeHost(ctx->h_out);
+    cudaFreeHost(ctx->h_init);
+    cudaFree(ctx->d_scratch);
+    cudaFree(ctx->d_data);
+    cudaFree(ctx->d_join);
+    cudaFreeHost(ctx->h_join);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+// ---------------------------------------------------------------------------
+// circuits and text
+
+extern "C" int nsat_circuit_new(nsat_ctx* ctx, const nsat_circuit_desc* desc, nsat_circuit** out) {
+    if (!ctx || !desc || !out || (desc->gate_num && !desc->gates) || !desc->outputs) return NSAT_EINVAL;
+    *out = nullptr;
+    for (uint32_t k = 0; k < desc->gate_num; k++)
+        if (desc->gates[3 * k] > 3) return fail(ctx, NSAT_EINVAL, "bad gate function");
+    Circuit c = from_desc(desc);
+    std::string v = c.validate();
+    if (!v.empty()) return fail(ctx, NSAT_EINVAL, v);
+    nsat_circuit* nc = new nsat_circuit();
+    nc->ctx = ctx;
+    nc->circ = std::move(c);
+    *out = nc;
+    return NSAT_OK;
+}
+
+extern "C" void nsat_circuit_free(nsat_circuit* c) { delete c; }
+
+extern "C" int nsat_circuit_stats(nsat_ctx* ctx, nsat_circuit* c, int output, uint32_t* live,
+                                  uint32_t* ops) {
+    if (!ctx || !c) return NSAT_EINVAL;
+    std::vector<uint32_t> which;
+    if (output < 0) for (uint32_t j = 0; j < c->circ.outputs.size(); j++) which.push_back(j);
+    else if ((size_t)output < c->circ.outputs.size()) which.push_back((uint32_t)output);
+    else return NSAT_EINVAL;
+    const LutNet& net = get_net(c, which);
+    if (live) *live = net.live_gates;
+    if (ops) *ops = (uint32_t)net.luts.size();
+    return NSAT_OK;
+}
+
+extern "C" int nsat_parse(const char* text, size_t len, nsat_parsed** out) {
+    if (!text || !out) return NSAT_EINVAL;
+    *out = nullptr;
+    std::unique_ptr<nsat_parsed> p(new nsat_parsed());
+    std::string err;
+    if (!parse_gatesim(std::string(text, len), &p->p, &err)) return NSAT_EPARSE;
+    for (const Gate& g : p->p.circuit.gates) { p->gates.push_back(g.func); p->gates.push_back(g.i0); p->gates.push_back(g.i1); }
+    for (const Output& o : p->p.circuit.outputs) { p->outputs.push_back(o.wire); p->outputs.push_back(o.neg); }
+    *out = p.release();
+    return NSAT_OK;
+}
+
+extern "C" int nsat_parsed_get(const nsat_parsed* p, nsat_circuit_desc* d, const uint8_t** quants) {
+    if (!p || !d) return NSAT_EINVAL;
+    d->input_len = p->p.circuit.n;
+    d->gate_num = (uint32_t)p->p.circuit.gates.size();
+    d->gates = p->gates.data();
+    d->output_num = (uint32_t)p->p.circuit.outputs.size();
+    d->outputs = p->outputs.data();
+    if (quants) *quants = p->p.quants.empty() ? nullptr : p->p.quants.data();
+    return NSAT_OK;
+}
+
+extern "C" void nsat_parsed_free(nsat_parsed* p) { delete p; }
+
+extern "C" int nsat_format(const nsat_circuit_desc* desc, const uint8_t* quants, char* buf, size_t buflen,
+                           size_t* needed) {
+    if (!desc) return NSAT_EINVAL;
+    Circuit c = from_desc(desc);
+    if (!c.validate().empty()) return NSAT_EINVAL;
+    std::vector<uint8_t> q;
+    if (quants) q.assign(quants, quants + c.n);
+    std::string s = format_gatesim(c, quants ? &q : nullptr);
+    if (needed) *needed = s.size();
+    if (buf && buflen) {
+        size_t k = std::min(buflen - 1, s.size());
+        memcpy(buf, s.data(), k);
+        buf[k] = 0;
+        if (k < s.size()) return NSAT_EINVAL;
+    }
+    return NSAT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// SAT
+
+extern "C" int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opts* opts,
+                              nsat_sat_result* res) {
+    if (!ctx || !c || !res) return NSAT_EINVAL;
+    memset(res, 0, sizeof(*res));
+    const double t_start = now_ms();
+    if (int rc = set_device(ctx)) return rc;
+    nsat_sat_opts o{};
+    if (opts) o = *opts;
+    SatPlan plan;
+    std::string perr;
+    if (int rc = plan_sat(c->circ.n, o, ctx->opts.block_threads, &plan, &perr)) return fail(ctx, rc, perr);
+    const KernelConfig& kc = plan.kc;
+    const uint32_t d = plan.d, C = plan.C;
+    const u128 bp = plan.bp, ep = plan.ep;
+    const std::vector<uint32_t> out0{0};
+    const LutNet& net = get_net(c, out0);
+    CUfunction fn;
+    std::shared_ptr<JitModule> mod;
+    if (int rc = get_kernel(ctx, kc, net, "nsat_sat", &fn, &mod)) return rc;
+    const uint64_t L0 = (uint64_t)(bp >> C);
+    const uint64_t nl = (uint64_t)((ep - bp) >> C);
+    const unsigned grid = 1u << kc.cb, threads = kc.threads();
+    u128 count = 0;
+    bool found = false;
+    u128 witness = 0;
+    uint64_t consumed = 0;
+    double dev_ms = 0;
+    uint32_t launches = 0;
+    uint64_t launch_idx_buf[kRing];
+    LaunchOut* d_out = ctx->d_out;
+    int rc = run_ring(
+        ctx, nl,
+        [&](uint64_t k, int slot) {
+            launch_idx_buf[slot] = L0 + k;
+            LaunchOut* po = d_out + slot;
+            void* params[] = {&launch_idx_buf[slot], &po};
+            return launch(ctx, fn, grid, threads, params);
+        },
+        [&](uint64_t k, const LaunchOut& r) {
+            consumed = k + 1;
+            count += r.count;
+            if (r.min_idx != ~0ull && !found) {
+                found = true;
+                witness = (((u128)(L0 + k)) << C) + r.min_idx;
+            }
+            return !(found && !o.find_all);
+        },
+        &dev_ms, &launches);
+    if (rc) return rc;
+    res->satisfiable = found ? 1 : 0;
+    const u128 cnt = count >> d;
+    res->count_lo = (uint64_t)cnt;
+    res->count_hi = (uint64_t)(cnt >> 64);
+    const u128 w = witness >> d;
+    res->witness_lo = found ? (uint64_t)w : 0;
+    res->witness_hi = found ? (uint64_t)(w >> 64) : 0;
+    const u128 sc = ((u128)consumed << C) >> d;
+    res->scanned_lo = (uint64_t)sc;
+    res->scanned_hi = (uint64_t)(sc >> 64);
+    res->device_ms = dev_ms;
+    res->launches = launches;
+    res->wall_ms = now_ms() - t_start;
+    return NSAT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// QSAT
+
+namespace {
+
+int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quants_in,
+                const uint32_t* data_words, uint32_t n_items_bits, uint32_t chunk_bits,
+                nsat_qsat_result* res) {
+    memset(res, 0, sizeof(*res));
+    const double t_start = now_ms();
+    if (int rc = set_device(ctx)) return rc;
+    const bool data = data_words != nullptr;
+    const uint32_t n = data ? n_items_bits : c->circ.n;
+    QsatPlan plan;
+    std::string perr;
+    if (int rc = plan_qsat(n, quants_in, data, chunk_bits, ctx->opts.block_threads, &plan, &perr))
+        return fail(ctx, rc, perr);
+    const KernelConfig& kc = plan.kc;
+    const std::vector<uint8_t>& q = plan.q;
+    const uint32_t d = plan.d, np = plan.np, f = plan.f, m = plan.m, C = plan.C, A = plan.A;
+    LutNet empty;
+    const std::vector<uint32_t> out0{0};
+    const LutNet& net = data ? empty : get_net(c, out0);
+    CUfunction fn;
+    std::shared_ptr<JitModule> mod;
+    if (int rc = get_kernel(ctx, kc, net, "nsat_qsat", &fn, &mod)) return rc;
+    if (int rc = ensure_scratch(ctx, (size_t)2 << kc.cb)) return rc;
+    if (data) {
+        // expand 2^n items to 2^np (each item repeated 2^d times)
+        const uint64_t nw = 1ull << (np - 5);
+        std::vector<uint32_t> ex(nw, 0);
+        for (uint64_t v = 0; v < (1ull << np); v++) {
+            uint64_t src = v >> d;
+            if ((data_words[src >> 5] >> (src & 31)) & 1u) ex[v >> 5] |= 1u << (v & 31);
+        }
+        if (ctx->data_bytes < nw * 4) {
+            cudaFree(ctx->d_data);
+            ctx->d_data = nullptr;
+            ctx->data_bytes = 0;
+            CK(cudaMalloc(&ctx->d_data, nw * 4));
+            ctx->data_bytes = nw * 4;
+        }
+        CK(cudaMemcpyAsync(ctx->d_data, ex.data(), nw * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    const bool q0all = q[0] != 0;
+    const bool dec = !q0all;   // value of a decisive unit
+    std::unique_ptr<QuantReducer> qr;
+    if (A > 0) qr.reset(new QuantReducer(std::vector<uint8_t>(q.begin(), q.begin() + A)));
+    FinalResult fr;
+    bool have = false;
+    uint64_t nl = A == 64 ? ~0ull : (1ull << A);
+    const unsigned grid = 1u << kc.cb, threads = kc.threads();
+    uint64_t launch_idx_buf[kRing];
+    LaunchOut* d_out = ctx->d_out;
+    unsigned char* scratch = ctx->d_scratch;
+    const uint32_t* dd = ctx->d_data;
+    double dev_ms = 0;
+    uint32_t launches = 0;
+    int rc = run_ring(
+        ctx, nl,
+        [&](uint64_t k, int slot) {
+            launch_idx_buf[slot] = k;
+            LaunchOut* po = d_out + slot;
+            void* params[] = {&launch_idx_buf[slot], &po, &scratch, &dd};
+            return launch(ctx, fn, grid, threads, params);
+        },
+        [&](uint64_t k, const LaunchOut& r) {
+            if (A == 0) {
+                fr.reversed = q0all;
+                fr.solution_bits = f;
+                fr.has_solution = r.min_idx != ~0ull;
+                fr.solution = fr.has_solution ? reverse_bits(r.min_idx, f) : 0;
+                have = true;
+                return false;
+            }
+            bool value;
+            if (m < C) value = (r.min_idx != ~0ull) ? dec : !dec;
+            else value = r.tree != 0;
+            qr->push(value);
+            FinalResult t;
+            if (qr->final_result(&t)) {
+                fr.reversed = q0all;
+                fr.solution_bits = f;
+                fr.has_solution = t.has_solution;
+                if (t.has_solution && f > A)
+                    fr.solution = t.solution | (reverse_bits(r.min_idx, f - A) << A);
+                else
+                    fr.solution = t.has_solution ? t.solution : 0;
+                have = true;
+                (void)k;
+                return false;
+            }
+            return true;
+        },
+        &dev_ms, &launches);
+    if (rc) return rc;
+    if (!have) return fail(ctx, NSAT_ECUDA, "QSAT reduction did not finish");
+    res->reversed = fr.reversed;
+    res->solution_bits = fr.solution_bits;
+    res->has_solution = fr.has_solution;
+    res->value = fr.has_solution ? (q0all ? 0 : 1) : (q0all ? 1 : 0);
+    res->solution_lo = fr.solution;
+    res->solution_hi = 0;
+    res->launches = launches;
+    res->device_ms = dev_ms;
+    res->wall_ms = now_ms() - t_start;
+    return NSAT_OK;
+}
+
+}  // namespace
+
+extern "C" int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
+                               const nsat_qsat_opts* opts, nsat_qsat_result* res) {
+    if (!ctx || !c || !quants || !res) return NSAT_EINVAL;
+    std::vector<uint8_t> q(quants, quants + c->circ.n);
+    for (auto& v : q) v = v ? 1 : 0;
+    uint32_t f = 0;
+    while (f < q.size() && q[f] == q[0]) f++;
+    if (f > 64) return fail(ctx, NSAT_EUNSUPPORTED, "first quantifier block longer than 64");
+    return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res);
+}
+
+extern "C" int nsat_qsat_reduce_words(nsat_ctx* ctx, const uint8_t* quants, uint32_t nq,
+                                      const uint32_t* words, nsat_qsat_result* res) {
+    if (!ctx || !quants || !words || !res || nq < 5 || nq > 30) return NSAT_EINVAL;
+    std::vector<uint8_t> q(quants, quants + nq);
+    for (auto& v : q) v = v ? 1 : 0;
+    return qsat_common(ctx, nullptr, q, words, nq, 0, res);
+}
+
+// ---------------------------------------------------------------------------
+// SATOSTOP
+
+extern "C" int nsat_stop_table_build(nsat_ctx* ctx, nsat_circuit* c, const nsat_table_opts* opts,
+                                     nsat_table** out) {
+    if (!ctx || !c || !out) return NSAT_EINVAL;
+    *out = nullptr;
+    if (int rc = set_device(ctx)) return rc;
+    const uint32_t n = c->circ.n;
+    KernelConfig kc;
+    std::string perr;
+    if (int rc = plan_table(c->circ, opts && opts->want_steps, &kc, &perr)) return fail(ctx, rc, perr);
+    std::unique_ptr<nsat_table> t(new nsat_table());
+    t->ctx = ctx;
+    t->n = n;
+    t->fmt = kc.fmt;
+    t->N = 1ull << n;
+    t->entry_bytes = kc.fmt == 0 ? 4 : 8;
+    const size_t bytes = std::max<size_t>(t->N * t->entry_bytes, 256);
+    for (int i = 0; i < 2; i++) {
+        cudaError_t e = cudaMalloc(&t->buf[i], bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, NSAT_ENOMEM, "table allocation failed");
+        }
+    }
+    std::vector<uint32_t> which;
+    for (uint32_t j = 0; j <= n; j++) which.push_back(j);
+    const LutNet& net = get_net(c, which);
+    CUfunction fn;
+    std::shared_ptr<JitModule> mod;
+    if (int rc = get_kernel(ctx, kc, net, "nsat_table", &fn, &mod)) return rc;
+    uint64_t nwords = n >= 5 ? (t->N >> 5) : 1;
+    const unsigned threads = kc.threads();
+    uint64_t want = (nwords + threads - 1) / threads;
+    unsigned grid = (unsigned)std::min<uint64_t>(want, (uint64_t)ctx->sm_count * 16);
+    LaunchOut* po = ctx->d_out;
+    void* tb = t->buf[0];
+    void* params[] = {&nwords, &tb, &po};
+    CK(cudaMemcpyAsync(ctx->d_out, ctx->h_init, sizeof(LaunchOut), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaEventRecord(ctx->ev0[0], ctx->stream));
+    if (int rc = launch(ctx, fn, grid, threads, params)) return rc;
+    CK(cudaEventRecord(ctx->ev1[0], ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_out, ctx->d_out, sizeof(LaunchOut), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0[0], ctx->ev1[0]));
+    t->build_ms = ms;
+    t->any_stop = ctx->h_out[0].any != 0;
+    t->cur = 0;
+    *out = t.release();
+    return NSAT_OK;
+}
+
+extern "C" void nsat_table_free(nsat_table* t) { delete t; }
+
+extern "C" uint64_t nsat_table_bytes(const nsat_table* t) {
+    return t ? 2ull * std::max<uint64_t>(t->N * t->entry_bytes, 256) : 0;
+}
+
+extern "C" int nsat_table_read(nsat_table* t, uint64_t first, uint64_t count, uint64_t* out) {
+    if (!t || !out || first > t->N || count > t->N - first) return NSAT_EINVAL;
+    nsat_ctx* ctx = t->ctx;
+    if (int rc = set_device(ctx)) return rc;
+    const uint64_t mask = (t->fmt == 2) ? 0xffffffffull : ~0ull;
+    if (t->entry_bytes == 4) {
+        std::vector<uint32_t> tmp(count);
+        CK(cudaMemcpy(tmp.data(), (uint32_t*)t->buf[t->cur] + first, count * 4, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < count; i++) out[i] = tmp[i];
+    } else {
+        CK(cudaMemcpy(out, (uint64_t*)t->buf[t->cur] + first, count * 8, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < count; i++) out[i] &= mask;
+    }
+    return NSAT_OK;
+}
+
+extern "C" int nsat_stop_solve(nsat_ctx* ctx, nsat_table* t, const nsat_stop_opts* opts,
+                               nsat_stop_result* res) {
+    if (!ctx || !t || !opts || !res || t->ctx != ctx) return NSAT_EINVAL;
+    memset(res, 0, sizeof(*res));
+    if (opts->unknowns > t->n || opts->mode > 1) return NSAT_EINVAL;
+    if (int rc = set_device(ctx)) return rc;
+    res->build_ms = t->build_ms;
+    if (!t->any_stop) return NSAT_OK;   // check_stop: no state ever stops
+    NsatJoinState* h = ctx->h_join;
+    memset(h, 0, sizeof(*h));
+    for (int i = 0; i < 72; i++) h->best[i] = ~0ull;
+    CK(cudaMemcpyAsync(ctx->d_join, h, sizeof(*h), cudaMemcpyHostToDevice, ctx->stream));
+    const uint32_t n = t->n;
+    CK(cudaEventRecord(ctx->ev0[0], ctx->stream));
+    int src = t->cur;
+    for (uint32_t r = 1; r <= n; r++) {
+        int rc = nsat_launch_join_round((int)t->fmt, t->buf[src], t->buf[src ^ 1], t->N, n, opts->unknowns, r,
+                                        opts->mode, ctx->d_join, ctx->sm_count, ctx->stream);
+        if (rc) return fail(ctx, NSAT_ECUDA, "join launch failed");
+        src ^= 1;
+    }
+    CK(cudaEventRecord(ctx->ev1[0], ctx->stream));
+    CK(cudaMemcpyAsync(h, ctx->d_join, sizeof(*h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0[0], ctx->ev1[0]));
+    res->join_ms = ms;
+    const uint32_t fr = h->final_round ? h->final_round : n;
+    const uint64_t best = h->best[fr];
+    res->rounds = fr;
+    // round r wrote buffer cur0 ^ (r & 1); rounds after an early exit write nothing
+    const int buf = t->cur ^ (int)(fr & 1);
+    t->cur = buf;
+    if (best != ~0ull) {
+        uint64_t e = 0;
+        if (t->entry_bytes == 4) {
+            uint32_t v;
+            CK(cudaMemcpy(&v, (uint32_t*)t->buf[buf] + best, 4, cudaMemcpyDeviceToHost));
+            e = v;
+        } else {
+            CK(cudaMemcpy(&e, (uint64_t*)t->buf[buf] + best, 8, cudaMemcpyDeviceToHost));
+        }
+        res->found = 1;
+        res->start = best;
+        res->end = e & ((1ull << n) - 1);
+        res->steps = t->fmt == 2 ? (e >> 32) : 0;
+    }
+    return NSAT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// measurement
+
+extern "C" int nsat_probe_lop3_peak(nsat_ctx* ctx, double* lop3_per_s, double* sm_mhz) {
+    if (!ctx || !lop3_per_s) return NSAT_EINVAL;
+    if (int rc = set_device(ctx)) return rc;
+    const int blocks = ctx->sm_count * 8, iters = 1 << 14;
+    uint32_t* dbuf = nullptr;
+    uint64_t* dclk = nullptr;
+    CK(cudaMalloc(&dbuf, (size_t)blocks * 256 * 4));
+    CK(cudaMalloc(&dclk, 8));
+    double best = 0, mhz = 0;
+    for (int rep = 0; rep < 3; rep++) {
+        CK(cudaEventRecord(ctx->ev0[0], ctx->stream));
+        if (nsat_launch_lop3_probe(dbuf, blocks, iters, dclk, ctx->stream)) {
+            cudaFree(dbuf); cudaFree(dclk);
+            return fail(ctx, NSAT_ECUDA, "probe launch failed");
+        }
+        CK(cudaEventRecord(ctx->ev1[0], ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0[0], ctx->ev1[0]));
+        uint64_t clk = 0;
+        CK(cudaMemcpy(&clk, dclk, 8, cudaMemcpyDeviceToHost));
+        const double ops = (double)blocks * 256.0 * iters * 16.0;
+        const double rate = ops / (ms * 1e-3);
+        if (rate > best) { best = rate; mhz = (double)clk / (ms * 1e3); }
+    }
+    cudaFree(dbuf);
+    cudaFree(dclk);
+    *lop3_per_s = best;
+    if (sm_mhz) *sm_mhz = mhz;
+    return NSAT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// build check (no device needed)
+
+extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quants, int kind,
+                              const nsat_opts* opts, nsat_jit_info* info, char* log, size_t loglen) {
+    if (!desc || !info || kind < 0 || kind > 2) return NSAT_EINVAL;
+    memset(info, 0, sizeof(*info));
+    for (uint32_t k = 0; k < desc->gate_num; k++)
+        if (desc->gates[3 * k] > 3) return NSAT_EINVAL;
+    Circuit c = from_desc(desc);
+    if (!c.validate().empty()) return NSAT_EINVAL;
+    const bool raw = opts && opts->no_optimize;
+    const uint32_t bt = opts ? opts->block_threads : 0;
+    KernelConfig kc;
+    std::vector<uint32_t> which{0};
+    std::string err;
+    int rc;
+    if (kind == 0) {
+        SatPlan pl;
+        nsat_sat_opts so{};
+        so.find_all = 1;
+        rc = plan_sat(c.n, so, bt, &pl, &err);
+        kc = pl.kc;
+    } else if (kind == 1) {
+        if (!quants) return NSAT_EINVAL;
+        std::vector<uint8_t> q(quants, quants + c.n);
+        for (auto& v : q) v = v ? 1 : 0;
+        QsatPlan pl;
+        rc = plan_qsat(c.n, q, false, 0, bt, &pl, &err);
+        kc = pl.kc;
+    } else {
+        rc = plan_table(c, false, &kc, &err);
+        which.clear();
+        for (uint32_t j = 0; j < c.outputs.size(); j++) which.push_back(j);
+    }
+    if (rc) return rc;
+    LutNet net = map_luts(c, which, raw);
+    info->lop3_ops = (uint32_t)net.luts.size();
+    info->live_gates = net.live_gates;
+    std::string src = generate_source(kc, net);
+    std::string clog;
+    double ms = 0;
+    rc = jit_compile_only(src, &clog, &ms, &err);
+    info->compile_ms = ms;
+    const std::string& text = rc ? err : clog;
+    if (log && loglen) {
+        size_t k = std::min(loglen - 1, text.size());
+        memcpy(log, text.data(), k);
+        log[k] = 0;
+    }
+    if (rc) return NSAT_ECOMPILE;
+    // ptxas -v: "Used N registers" and "N bytes spill stores"
+    size_t p = clog.find("Used ");
+    if (p != std::string::npos) info->regs = atoi(clog.c_str() + p + 5);
+    p = clog.find("bytes spill stores");
+    if (p != std::string::npos) {
+        size_t b = clog.rfind(',', p);
+        b = (b == std::string::npos) ? clog.rfind(' ', p - 2) : b + 1;
+        info->spill_bytes = atoi(clog.c_str() + b);
+    }
+    return NSAT_OK;
+}

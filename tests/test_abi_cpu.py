@@ -1,0 +1,104 @@
+"""Host-side checks that need no GPU: the C ABI loads and exports every
+declared symbol, text I/O round-trips, and every kernel kind NVRTC-compiles
+for sm_100a."""
+import os
+import re
+
+import pytest
+
+from naivesat_b200 import api
+from naivesat_b200 import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "nsat.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nsat_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = api.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(api.EXPORTS) <= set(syms)
+
+
+def test_no_device_is_reported_cleanly():
+    if api.device_count() > 0:
+        pytest.skip("a device is present")
+    with pytest.raises(api.NsatError, match="no CUDA device"):
+        api.Context(0)
+
+
+def test_strerror_codes():
+    L = api.lib()
+    for code in range(-9, 1):
+        assert L.nsat_strerror(code)
+
+
+def test_gatesim_text_roundtrip():
+    for name in ["c0", "c2a", "c3b"]:
+        c = W.config(name)
+        text = api.format_circuit(c.n, c.gates, c.outputs, c.quants)
+        n, gates, outs, quants = api.parse(text)
+        assert n == c.n
+        assert (gates == c.gates).all() and (outs == c.outputs).all()
+        assert quants == c.quants
+
+
+def test_gatesim_text_examples():
+    n, g, o, q = api.parse("{0 1 2 and(0,1) nor(2,3):0n xor(3,4):1}(3)")
+    assert n == 3 and g.tolist() == [[0, 0, 1], [1, 2, 3], [3, 3, 4]]
+    assert o.tolist() == [[4, 1], [5, 0]] and q is None
+    n, g, o, q = api.parse("ae a {0 1 2 nimpl(0,1):0}(3)")
+    assert q == "AEA" and g.tolist() == [[2, 0, 1]]
+    n, g, o, q = api.parse("{0:0 1:1n}(2)")     # identity outputs on inputs
+    assert o.tolist() == [[0, 0], [1, 1]]
+    for bad in ["{0 1 and(0,5):0}(2)", "{0 1 foo(0,1):0}(2)", "{0 1 and(0,1)}(2)", "{0:1}(1)"]:
+        with pytest.raises(api.NsatError):
+            api.parse(bad)
+
+
+def test_negation_folding_preserves_function():
+    """The generators fold negated fan-ins into gatesim gates; the folded
+    circuit must compute what the raw gates describe."""
+    rng = W.SplitMix64(5)
+    for t in range(20):
+        n = 6
+        rb = W.random_dag_raw(rng, n, 40, window=8)
+        rb.output(n + 39)
+        rb.output(n + 20, 1)
+        c = rb.fold()
+        for v in range(1 << n):
+            bits = [(v >> i) & 1 for i in range(n)]
+            w = bits + [0] * len(rb.raw)
+            for k, (f, a, na, b, nb) in enumerate(rb.raw):
+                w[n + k] = W._gate(f, w[a] ^ na, w[b] ^ nb)
+            exp = [w[n + 39], w[n + 20] ^ 1]
+            assert c.eval_bits(bits) == exp
+
+
+@pytest.mark.parametrize("name,kind", [("c0", "sat"), ("c2a", "qsat"), ("c3b", "table"),
+                                       ("c3a", "table")])
+def test_kernels_compile_for_sm100a(name, kind):
+    c = W.config(name)
+    r = api.jit_check(c, kind, quants=c.quants)
+    assert r["regs"] > 0, r["log"]
+    assert r["spill_bytes"] == 0, r["log"]
+    assert r["lop3_ops"] <= r["live_gates"]
+
+
+def test_one_op_per_gate_mode_compiles():
+    c = W.config("c0")
+    r = api.jit_check(c, "sat", no_optimize=True)
+    assert r["lop3_ops"] == r["live_gates"]
+
+
+def test_lut_mapping_saves_ops():
+    c = W.config("c1")
+    fused = api.jit_check(c, "sat")
+    assert fused["lop3_ops"] < 0.8 * fused["live_gates"], fused
