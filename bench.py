@@ -182,7 +182,7 @@ def run_ours(args, world, rank, local):
 
     circ = W.config(WORKLOAD)
     n = circ.n
-    total = 1 << n
+    total = 1 << min(n, args.log2)
     per = total // world
     begin, end = rank * per, (rank + 1) * per
     ctx = api.Context(local)
@@ -272,7 +272,7 @@ def run_ours(args, world, rank, local):
                      "frac": lop3_rate / peak_lop3, "traffic": None,
                      "peak_source": "measured lop3.b32 chain microbenchmark on this GPU "
                                     "(nsat_probe_lop3_peak, %.0f MHz)" % probe_mhz},
-        "cpu_baseline": cpu_baseline(circ),
+        "cpu_baseline": cpu_baseline(circ) if not args.no_cpu_baseline else None,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": int(32 * launches_per_step),
                 "d2h_bytes_per_step": int(32 * launches_per_step)},
         "gpu_launches": launches,
@@ -288,6 +288,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log2", type=int, default=36,
+                    help="enumerate only the first 2^LOG2 assignments (smaller cases for profiling)")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     try:

@@ -828,7 +828,8 @@ extern "C" int nsat_probe_lop3_peak(nsat_ctx* ctx, double* lop3_per_s, double* s
     uint32_t* dbuf = nullptr;
     uint64_t* dclk = nullptr;
     CK(cudaMalloc(&dbuf, (size_t)blocks * 256 * 4));
-    CK(cudaMalloc(&dclk, 8));
+    CK(cudaMalloc(&dclk, 24 * (size_t)blocks));
+    std::vector<uint64_t> hclk(3 * (size_t)blocks);
     double best = 0, mhz = 0;
     for (int rep = 0; rep < 3; rep++) {
         CK(cudaEventRecord(ctx->ev0[0], ctx->stream));
@@ -840,8 +841,19 @@ extern "C" int nsat_probe_lop3_peak(nsat_ctx* ctx, double* lop3_per_s, double* s
         CK(cudaStreamSynchronize(ctx->stream));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->ev0[0], ctx->ev1[0]));
-        uint64_t clk = 0;
-        CK(cudaMemcpy(&clk, dclk, 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hclk.data(), dclk, 24 * (size_t)blocks, cudaMemcpyDeviceToHost));
+        // per SM: cycles from the first block's loop start to the last
+        // block's loop end (clock64 is a per-SM counter), averaged over SMs
+        std::map<uint64_t, std::pair<uint64_t, uint64_t>> span;
+        for (int b = 0; b < blocks; b++) {
+            const uint64_t c0 = hclk[3 * b], c1 = hclk[3 * b + 1], sm = hclk[3 * b + 2];
+            auto it = span.find(sm);
+            if (it == span.end()) span[sm] = {c0, c1};
+            else { it->second.first = std::min(it->second.first, c0); it->second.second = std::max(it->second.second, c1); }
+        }
+        double cyc = 0;
+        for (auto& kv : span) cyc += (double)(kv.second.second - kv.second.first);
+        const uint64_t clk = span.empty() ? 0 : (uint64_t)(cyc / (double)span.size());
         const double ops = (double)blocks * 256.0 * iters * 16.0;
         const double rate = ops / (ms * 1e-3);
         if (rate > best) { best = rate; mhz = (double)clk / (ms * 1e3); }

@@ -114,7 +114,13 @@ __global__ void __launch_bounds__(256) lop3_probe(u32* out, int iters, u64* clk)
     u64 c1 = clock64();
     u32 r = a0 ^ a1 ^ a2 ^ a3 ^ a4 ^ a5 ^ a6 ^ a7;
     if (r == 0x12345678u) out[blockIdx.x * blockDim.x + threadIdx.x] = r;   // keeps the chains live
-    if (blockIdx.x == 0 && threadIdx.x == 0) *clk = c1 - c0;
+    if (threadIdx.x == 0) {
+        u32 smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        clk[3 * blockIdx.x] = c0;
+        clk[3 * blockIdx.x + 1] = c1;
+        clk[3 * blockIdx.x + 2] = smid;
+    }
 }
 
 }  // namespace

@@ -1,0 +1,99 @@
+"""The four command-line tools: argument handling (CPU) and end-to-end
+answers on circuit files (GPU), in the reference's output formats."""
+import os
+import subprocess
+
+import pytest
+
+from naivesat_b200 import api
+from naivesat_b200 import workloads as W
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "naivesat_b200", "bin")
+TOOLS = ["naivesat", "naiveqsat", "naivesatostop", "greedysatostop"]
+
+
+def run(tool, *args, check=False):
+    p = subprocess.run([os.path.join(BIN, tool)] + [str(a) for a in args], capture_output=True,
+                       text=True, timeout=600)
+    if check:
+        assert p.returncode == 0, p.stdout + p.stderr
+    return p
+
+
+def write(tmp_path, circ, name):
+    path = tmp_path / (name + ".circuit")
+    path.write_text(api.format_circuit(circ.n, circ.gates, circ.outputs, circ.quants))
+    return path
+
+
+@pytest.mark.parametrize("tool", TOOLS)
+def test_help_and_bad_args(tool):
+    p = run(tool, "--help")
+    assert p.returncode == 0 and "Usage:" in p.stdout
+    p = run(tool, "--bogus-flag", "x")
+    assert p.returncode == 2
+    p = run(tool, "/nonexistent.circuit", "3", "-t", "opencl:0")
+    assert p.returncode != 0
+
+
+def test_exec_type_is_required(tmp_path):
+    path = write(tmp_path, W.config("c0"), "c0")
+    p = run("naivesat", path)
+    assert p.returncode == 2 and "exec-type" in p.stderr
+
+
+gpu = pytest.mark.gpu
+
+
+def bits(v, n):
+    return format(v, "0%db" % n)
+
+
+@gpu
+def test_naivesat_cli(tmp_path):
+    c = W.config("c0")
+    cnt, low = O.sat_range(O.Circuit(c.n, c.gates, c.outputs))
+    out = run("naivesat", write(tmp_path, c, "c0"), "-t", "opencl:0", check=True).stdout
+    assert "Found Input: %s\n" % bits(low, c.n) in out
+    out = run("naivesat", write(tmp_path, c, "c0"), "-t", "cpu_and_opencl", "-e", "20", check=True).stdout
+    assert "Found Input: %s\n" % bits(low, c.n) in out
+    unsat = W.Circuit(16, [(W.NIMPL, 3, 3)], [(16, 0)])
+    out = run("naivesat", write(tmp_path, unsat, "u"), "-t", "opencl:0", check=True).stdout
+    assert out.rstrip().endswith("Unsatisfiable!")
+    small = W.random_dag(3, 10, 40, output="live")
+    cnt, low = O.sat_range(O.Circuit(small.n, small.gates, small.outputs))
+    out = run("naivesat", write(tmp_path, small, "s"), "-t", "opencl:0", check=True).stdout
+    assert ("Found Input: %s\n" % bits(low, 10)) in out if low is not None else "Unsatisfiable!" in out
+
+
+@gpu
+def test_naiveqsat_cli(tmp_path):
+    out = run("naiveqsat", write(tmp_path, W.config("c2a"), "a"), "-t", "opencl:0", check=True).stdout
+    assert "Result: (Satisfiable)\n" in out
+    out = run("naiveqsat", write(tmp_path, W.config("c2b"), "b"), "-t", "opencl:0", check=True).stdout
+    assert "Result: (Unsatisfiable: %s)\n" % ("0" * 16) in out
+    # plain circuit: every input existential (qsat.rs:6277-6285)
+    c = W.random_dag(5, 16, 120, output="live")
+    exp = O.qsat(O.Circuit(c.n, c.gates, c.outputs), "E" * 16)
+    out = run("naiveqsat", write(tmp_path, c, "p"), "-t", "cpu", check=True).stdout
+    if exp["solution"] is None:
+        assert "Result: (Unsatisfiable)\n" in out
+    else:
+        assert "Result: (Satisfiable: %s)\n" % bits(exp["solution"], 16) in out
+
+
+@gpu
+def test_satostop_clis(tmp_path):
+    path = write(tmp_path, W.config("c3b"), "cnt")
+    out = run("greedysatostop", path, 16, "-v", check=True).stdout
+    assert "Solution: Solution { start: 16776960, end: 0 }\n" in out
+    assert "Verified: end=0\n" in out and "INCORRECT" not in out
+    out = run("naivesatostop", path, 16, "-t", "opencl:0", "-v", check=True).stdout
+    assert "Solution: Solution { start: 0, end: 0, steps: 16777216 }\n" in out
+    assert "Verified: end=0 steps=16777216\n" in out and "INCORRECT" not in out
+    out = run("naivesatostop", path, 16, "-S", check=True).stdout
+    assert "Stopped at %s %s\n" % ("0" * 16, "0" * 24) in out
+    out = run("greedysatostop", write(tmp_path, W.config("c3a"), "lfsr"), 16, check=True).stdout
+    assert "Unsatisfiable!" in out
