@@ -144,6 +144,26 @@ typedef struct {
 int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
                     const nsat_qsat_opts* opts, nsat_qsat_result* res);
 
+/* nsat_qsat_solve for callers that cannot call cudaMalloc -- for example a
+ * serving process whose device memory belongs to another allocator or a fixed
+ * budget, where cudaMalloc/cudaFree would synchronize the device or break the
+ * budget mid-request.  No counterpart in the reference (its OpenCL reducer
+ * allocates its buffers per solver, qsat.rs:1046-1064).
+ * The last-CTA scratch comes from a static device array of
+ * NSAT_NOALLOC_SCRATCH_BYTES (64 KiB) inside libnsat.so instead of the
+ * context's lazily allocated buffer; every GPU that loads the library holds it
+ * until exit.  A solve whose launches need more scratch (2 << CB bytes, CB =
+ * log2 CTAs per launch) fails with NSAT_EUNSUPPORTED; lower chunk_bits then.
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and the
+ * first call for a circuit/quantifier string compiles and loads its kernel;
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (several contexts on one device, or
+ * other threads) race on it and must be serialised by the caller.  Results
+ * equal nsat_qsat_solve's. */
+#define NSAT_NOALLOC_SCRATCH_BYTES (64u * 1024u)
+int nsat_qsat_solve_noalloc(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
+                            const nsat_qsat_opts* opts, nsat_qsat_result* res);
+
 /* Runs the QSAT reduction kernel on raw item bits instead of a circuit
  * (item k = bit k%32 of words[k/32], 2^nq items, nq >= 5): the analogue of
  * the reference's identity-circuit aggregator tests (qsat.rs:2629-3520). */

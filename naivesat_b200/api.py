@@ -82,6 +82,7 @@ EXPORTS = [
     "nsat_parsed_get", "nsat_parsed_free", "nsat_format", "nsat_sat_solve", "nsat_qsat_solve",
     "nsat_qsat_reduce_words", "nsat_stop_table_build", "nsat_table_free", "nsat_table_read",
     "nsat_table_bytes", "nsat_stop_solve", "nsat_probe_lop3_peak", "nsat_jit_check",
+    "nsat_qsat_solve_noalloc",
 ]
 
 _lib = None
@@ -116,6 +117,8 @@ def lib():
         L.nsat_sat_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(SatOpts), C.POINTER(SatResult)]
         L.nsat_qsat_solve.argtypes = [C.c_void_p, C.c_void_p, U8P, C.POINTER(QsatOpts),
                                       C.POINTER(QsatResult)]
+        L.nsat_qsat_solve_noalloc.argtypes = [C.c_void_p, C.c_void_p, U8P, C.POINTER(QsatOpts),
+                                              C.POINTER(QsatResult)]
         L.nsat_qsat_reduce_words.argtypes = [C.c_void_p, U8P, C.c_uint32, U32P, C.POINTER(QsatResult)]
         L.nsat_stop_table_build.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(TableOpts),
                                             C.POINTER(C.c_void_p)]
@@ -250,6 +253,16 @@ class CircuitHandle:
         r = QsatResult()
         self.ctx._check(lib().nsat_qsat_solve(self.ctx.h, self.h, q.ctypes.data_as(U8P), C.byref(o),
                                               C.byref(r)), "qsat_solve")
+        return _qsat_dict(r)
+
+    def qsat_noalloc(self, quants, chunk_bits=0):
+        """nsat_qsat_solve_noalloc: the same solve with no device allocation
+        (scratch from the library's static device array)."""
+        q = _quants_array(quants, self.n)
+        o = QsatOpts(chunk_bits, 0)
+        r = QsatResult()
+        self.ctx._check(lib().nsat_qsat_solve_noalloc(self.ctx.h, self.h, q.ctypes.data_as(U8P), C.byref(o),
+                                                      C.byref(r)), "qsat_solve_noalloc")
         return _qsat_dict(r)
 
     def stop_table(self, want_steps=False):

@@ -20,6 +20,7 @@
 #include "jit.h"
 #include "lutmap.h"
 #include "qreducer.h"
+#include "internal.h"
 #include "static_kernels.h"
 
 using namespace nsat;
@@ -568,7 +569,8 @@ namespace {
 
 int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quants_in,
                 const uint32_t* data_words, uint32_t n_items_bits, uint32_t chunk_bits,
-                nsat_qsat_result* res) {
+                nsat_qsat_result* res, unsigned char* fixed_scratch = nullptr,
+                size_t fixed_scratch_bytes = 0) {
     memset(res, 0, sizeof(*res));
     const double t_start = now_ms();
     if (int rc = set_device(ctx)) return rc;
@@ -587,7 +589,14 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     CUfunction fn;
     std::shared_ptr<JitModule> mod;
     if (int rc = get_kernel(ctx, kc, net, "nsat_qsat", &fn, &mod)) return rc;
-    if (int rc = ensure_scratch(ctx, (size_t)2 << kc.cb)) return rc;
+    if (fixed_scratch) {
+        if (((size_t)2 << kc.cb) > fixed_scratch_bytes)
+            return fail(ctx, NSAT_EUNSUPPORTED,
+                        "launch needs " + std::to_string((size_t)2 << kc.cb) + " scratch bytes, the fixed area holds " +
+                        std::to_string(fixed_scratch_bytes) + " (use smaller chunk_bits)");
+    } else if (int rc = ensure_scratch(ctx, (size_t)2 << kc.cb)) {
+        return rc;
+    }
     if (data) {
         // expand 2^n items to 2^np (each item repeated 2^d times)
         const uint64_t nw = 1ull << (np - 5);
@@ -616,7 +625,7 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     const unsigned grid = 1u << kc.cb, threads = kc.threads();
     uint64_t launch_idx_buf[kRing];
     LaunchOut* d_out = ctx->d_out;
-    unsigned char* scratch = ctx->d_scratch;
+    unsigned char* scratch = fixed_scratch ? fixed_scratch : ctx->d_scratch;
     const uint32_t* dd = ctx->d_data;
     double dev_ms = 0;
     uint32_t launches = 0;
@@ -682,6 +691,20 @@ extern "C" int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* qu
     while (f < q.size() && q[f] == q[0]) f++;
     if (f > 64) return fail(ctx, NSAT_EUNSUPPORTED, "first quantifier block longer than 64");
     return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res);
+}
+
+int nsat::ctx_device(const nsat_ctx* ctx) { return ctx ? ctx->device : -1; }
+
+int nsat::qsat_solve_with_scratch(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
+                                   const nsat_qsat_opts* opts, nsat_qsat_result* res,
+                                   unsigned char* scratch, size_t scratch_bytes) {
+    if (!ctx || !c || !quants || !res || !scratch) return NSAT_EINVAL;
+    std::vector<uint8_t> q(quants, quants + c->circ.n);
+    for (auto& v : q) v = v ? 1 : 0;
+    uint32_t f = 0;
+    while (f < q.size() && q[f] == q[0]) f++;
+    if (f > 64) return fail(ctx, NSAT_EUNSUPPORTED, "first quantifier block longer than 64");
+    return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res, scratch, scratch_bytes);
 }
 
 extern "C" int nsat_qsat_reduce_words(nsat_ctx* ctx, const uint8_t* quants, uint32_t nq,

@@ -1,0 +1,46 @@
+"""nsat_qsat_solve_noalloc: the QSAT solve for callers that cannot call
+cudaMalloc (a serving process whose device memory belongs to another
+allocator or a fixed budget, where cudaMalloc/cudaFree would synchronize the
+device or overrun the budget mid-request).  Its scratch is the library's
+static device array, so its answers must equal the allocating
+nsat_qsat_solve's, bit for bit, call after call (the array keeps the previous
+call's bytes).  This file is collected last on purpose."""
+import pytest
+
+from naivesat_b200 import api
+from naivesat_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("reversed", "solution_bits", "solution", "value")
+
+
+def cases():
+    # two-level first block over 24 inputs: the tree runs through every stage,
+    # the CTA level included (last-CTA tail in the static scratch)
+    c24 = W.random_dag(501, 24, 600, output="live")
+    yield c24, "EA" + "E" * 22, 0
+    yield c24, "A" + "E" * 23, 15          # 2^9 launches joined on the host
+    yield c24, W.alternating_quants(502, 24, 5), 0
+    adder = W.config("c2b")                # 32 inputs, known counterexample a = 0
+    yield adder, adder.quants, 0
+    yield adder, "E" * 16 + "A" * 16, 0
+
+
+def test_noalloc_matches_allocating_solve_twice():
+    with api.Context(0) as ctx:
+        for circ, quants, chunk in cases():
+            h = ctx.circuit(circ)
+            ref = h.qsat(quants, chunk_bits=chunk)
+            for call in range(2):
+                got = h.qsat_noalloc(quants, chunk_bits=chunk)
+                assert {k: got[k] for k in KEYS} == {k: ref[k] for k in KEYS}, (circ.name, quants, call)
+
+
+def test_noalloc_rejects_launches_beyond_the_fixed_area():
+    # one-warp CTAs over 2^36 assignments per launch need 2^16 CTAs:
+    # 2 << 16 = 128 KiB of scratch > 64 KiB
+    with api.Context(0, block_threads=32) as ctx:
+        h = ctx.circuit(W.config("c1"))
+        with pytest.raises(api.NsatError, match="EUNSUPPORTED"):
+            h.qsat_noalloc("E" * 36, chunk_bits=36)
