@@ -1,20 +1,25 @@
 #!/usr/bin/env python3
-"""Benchmark of the naivesat hot path on B200: exhaustive bit-sliced SAT
-enumeration of the 36-input / 3018-gate planted random-DAG circuit (seed 1),
-exact solution count plus lowest witness over all 2^36 assignments.
+"""Benchmark of the naivesat hot path on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c1|c0|c1_twin|c2a|c2b|c2c|c3a|c3b|c3s]
 
-One step = one full enumeration of the 2^36 index space (split evenly across
-the N ranks, each on its own GPU; a 3-word all-reduce combines count and
-witness).  `value` is device time (CUDA events around every kernel launch on
-the launching stream), `e2e` the same work through the C ABI call from host
-buffers (circuit upload, launches, result readback), both max over ranks.
-`--impl reference` times the oracle port of the reference's gatenative CPU
-path on this host's cores instead (rank 0 only).
+Default workload (c1): exhaustive bit-sliced SAT of the 36-input / 3018-gate
+planted random-DAG circuit (seed 1), exact solution count plus lowest witness
+over all 2^36 assignments.  One step = one full enumeration, the index space
+split evenly across the N ranks (one GPU each); a tiny all-reduce combines
+counts and times.  `value` is device time (CUDA events around every kernel
+launch on the launching stream), `e2e` the same work through the C ABI call
+from host buffers (circuit upload, launches, result readback); both are the
+max over ranks.  `--impl reference` times the oracle port of the reference's
+gatenative CPU path on this host's cores instead (rank 0 only).
+
+The other workloads print the same line shape for the QSAT (c2*) and
+SATOSTOP (c3*) paths; their steps are replicas on every rank.
 """
 import argparse
 import json
+import math
 import os
 import shutil
 import statistics
@@ -26,11 +31,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "c1"
-METRIC = "gate-evals/s"
 
-
-def dist_setup(args):
+def dist_setup():
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -55,7 +57,6 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = None
 
     def start(self):
         if not shutil.which("nvidia-smi"):
@@ -76,7 +77,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.f.close()
-        sm, mx, reasons = [], 0, set()
+        sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             p = [x.strip() for x in line.split(",")]
@@ -98,27 +99,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(circ, target_s=12.0):
-    """Oracle port (bit-sliced AVX2 interpreter, OpenMP over blocks) on a
-    bounded sample of the same index space, sized to ~target_s seconds."""
-    from oracle import oracle as O
-    oc = O.Circuit(circ.n, circ.gates, circ.outputs)
-    threads = os.cpu_count() or 1
-    bits = 24
-    t0 = time.perf_counter()
-    O.sat_range(oc, 0, 1 << bits, threads)
-    dt = time.perf_counter() - t0
-    while dt < target_s / 3 and bits < 34:
-        bits += 1
-        t0 = time.perf_counter()
-        O.sat_range(oc, 0, 1 << bits, threads)
-        dt = time.perf_counter() - t0
-    rate = (1 << bits) * circ.num_gates / dt
-    return {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": "first 2^%d assignments of the 2^36 space (%.1f s), gate-evals/s = "
-                      "2^%d x %d gates / time" % (bits, dt, bits, circ.num_gates)}
-
-
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -129,74 +109,269 @@ def cpu_model():
     return "unknown"
 
 
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# workloads
+
+class SatWorkload:
+    """Exhaustive SAT: count + lowest witness over 2^min(n, log2) assignments."""
+    metric = "gate-evals/s"
+    kind = "sat"
+
+    def __init__(self, name, log2):
+        from naivesat_b200 import workloads as W
+        self.name = name
+        self.circ = W.config(name)
+        self.total = 1 << min(self.circ.n, log2)
+
+    def describe(self):
+        c = self.circ
+        return {"workload": "naivesat %s: %d-input %d-gate random DAG (%s), exhaustive SAT over "
+                            "2^%d assignments, exact count + lowest witness"
+                            % (self.name, c.n, c.num_gates, c.name, int(math.log2(self.total))),
+                "inputs": c.n, "gates": c.num_gates, "assignments_per_step": self.total}
+
+    def setup(self, ctx, world, rank):
+        per = self.total // world
+        self.begin, self.end = rank * per, (rank + 1) * per
+        self.ctx = ctx
+        self.h = ctx.circuit(self.circ)
+        self.live, self.lop3 = self.h.stats()
+
+    def step(self, fresh=False):
+        h = self.ctx.circuit(self.circ) if fresh else self.h
+        r = h.sat(find_all=True, begin=self.begin, end=self.end)
+        return {"device_ms": r["device_ms"], "launches": r["launches"],
+                "sig": (r["count"], r["witness"]), "count": r["count"], "witness": r["witness"]}
+
+    def work(self):           # gate-evals per step (all ranks)
+        return self.total * self.circ.num_gates
+
+    def roofline(self, world, dev_ms_per_step, peak_lop3, probe_mhz):
+        words = (self.total // world) // 32
+        rate = words * self.lop3 / (dev_ms_per_step * 1e-3)
+        return {"bound": "alu", "achieved": rate, "peak": peak_lop3, "unit": "lop3/s",
+                "frac": rate / peak_lop3, "traffic": 212736,
+                "traffic_note": "dram bytes per launch from ncu on a 2^32 launch (instruction and "
+                                "parameter fetch only; the kernel reads no data)",
+                "peak_source": "measured lop3.b32 chain microbenchmark on this GPU (%.0f MHz)" % probe_mhz,
+                "lop3_per_word": self.lop3, "live_gates": self.live}
+
+    def cpu(self, threads, target_s=12.0):
+        from oracle import oracle as O
+        oc = O.Circuit(self.circ.n, self.circ.gates, self.circ.outputs)
+        bits = min(24, self.circ.n)
+        while True:
+            t0 = time.perf_counter()
+            O.sat_range(oc, 0, 1 << bits, threads)
+            dt = time.perf_counter() - t0
+            if dt > target_s / 3 or bits >= min(self.circ.n, 34):
+                break
+            bits += 1
+        return (1 << bits) * self.circ.num_gates / dt, "first 2^%d assignments (%.1f s)" % (bits, dt)
+
+
+class QsatWorkload:
+    """QSAT decision + first-block witness (early exit as the tree allows)."""
+    metric = "gate-evals/s"
+    kind = "qsat"
+
+    def __init__(self, name):
+        from naivesat_b200 import workloads as W
+        self.name = name
+        self.circ = W.config(name)
+
+    def describe(self):
+        c = self.circ
+        return {"workload": "naiveqsat %s: %d inputs, %d gates, quantifiers %s" % (self.name, c.n, c.num_gates,
+                                                                               c.quants),
+                "inputs": c.n, "gates": c.num_gates}
+
+    def setup(self, ctx, world, rank):
+        self.ctx = ctx
+        self.h = ctx.circuit(self.circ)
+        self.live, self.lop3 = self.h.stats()
+        self.scanned = None
+
+    def step(self, fresh=False):
+        h = self.ctx.circuit(self.circ) if fresh else self.h
+        r = h.qsat(self.circ.quants)
+        self.scanned = r["scanned"]
+        return {"device_ms": r["device_ms"], "launches": r["launches"],
+                "sig": (r["reversed"], r["solution_bits"], r["solution"]), "result": r}
+
+    def work(self):
+        return self.scanned * self.circ.num_gates
+
+    def roofline(self, world, dev_ms_per_step, peak_lop3, probe_mhz):
+        rate = (self.scanned // 32) * self.lop3 / (dev_ms_per_step * 1e-3)
+        return {"bound": "alu", "achieved": rate, "peak": peak_lop3, "unit": "lop3/s",
+                "frac": rate / peak_lop3, "traffic": None,
+                "peak_source": "measured lop3.b32 chain microbenchmark on this GPU (%.0f MHz)" % probe_mhz,
+                "lop3_per_word": self.lop3, "live_gates": self.live}
+
+    def cpu(self, threads, target_s=12.0):
+        from oracle import oracle as O
+        oc = O.Circuit(self.circ.n, self.circ.gates, self.circ.outputs)
+        t0 = time.perf_counter()
+        O.qsat(oc, self.circ.quants, mode=1, threads=threads)
+        dt = time.perf_counter() - t0
+        return (1 << self.circ.n) * self.circ.num_gates / dt, "full oracle solve (%.1f s)" % dt
+
+
+class StopWorkload:
+    """SATOSTOP: table build + synchronous doubling, both on the device."""
+    metric = "join GB/s"
+    kind = "stop"
+
+    def __init__(self, name, unknowns, mode, steps_counts):
+        from naivesat_b200 import workloads as W
+        self.name = name
+        if name == "c3s":
+            self.circ = W.lfsr_stop(4, 32, 300)
+        else:
+            self.circ = W.config(name)
+        self.u, self.mode, self.want_steps = unknowns, mode, steps_counts
+
+    def describe(self):
+        c = self.circ
+        return {"workload": "SATOSTOP %s: %d-bit state, %d unknowns, %d gates, table + pointer doubling "
+                            "(mode %d)" % (self.name, c.n, self.u, c.num_gates, self.mode),
+                "state_bits": c.n, "unknowns": self.u, "gates": c.num_gates,
+                "entry_bytes": 8 if (self.want_steps or c.n > 31) else 4}
+
+    def setup(self, ctx, world, rank):
+        self.ctx = ctx
+        self.h = ctx.circuit(self.circ)
+        self.rounds = None
+        self.eb = 8 if (self.want_steps or self.circ.n > 31) else 4
+
+    def step(self, fresh=False):
+        h = self.ctx.circuit(self.circ) if fresh else self.h
+        t = h.stop_table(want_steps=self.want_steps)
+        r = t.solve(self.u, mode=self.mode)
+        del t
+        self.rounds = r["rounds"]
+        self.join_ms = r["join_ms"]
+        self.build_ms = r["build_ms"]
+        return {"device_ms": r["build_ms"] + r["join_ms"], "launches": 1 + self.circ.n,
+                "sig": (r["found"], r.get("start"), r.get("end"), r.get("steps"), r["rounds"]), "result": r}
+
+    def join_bytes(self):
+        return self.rounds * (1 << self.circ.n) * 3 * self.eb
+
+    def work(self):
+        return self.join_bytes() / 1e9
+
+    def roofline(self, world, dev_ms_per_step, peak_lop3, probe_mhz):
+        peak, src = measured_hbm_gbs()
+        ach = self.join_bytes() / (self.join_ms * 1e-3) / 1e9
+        return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "traffic": None, "peak_source": "%s hbm_gbs (MEASURED_PEAKS.json)" % src,
+                "kernel": "join_round", "algorithmic_bytes_per_entry_round": 3 * self.eb,
+                "rounds": self.rounds, "join_ms": self.join_ms, "build_ms": self.build_ms}
+
+    def cpu(self, threads, target_s=12.0):
+        from oracle import oracle as O
+        if self.circ.n > 26:
+            return None, "state too large for the host oracle"
+        oc = O.Circuit(self.circ.n, self.circ.gates, self.circ.outputs)
+        t0 = time.perf_counter()
+        tb = O.stop_table(oc, threads)
+        r = O.stop_solve(self.circ.n, self.u, tb, mode=self.mode, threads=threads)
+        dt = time.perf_counter() - t0
+        rounds = r["rounds"] if r else self.circ.n
+        bytes_ = rounds * (1 << self.circ.n) * 3 * 8
+        return bytes_ / dt / 1e9, "full oracle table + doubling (%.1f s, u64 arrays)" % dt
+
+
+def make_workload(name, log2):
+    if name in ("c0", "c1", "c1_twin"):
+        return SatWorkload(name, log2)
+    if name in ("c2a", "c2b", "c2c"):
+        return QsatWorkload(name)
+    if name in ("c3a", "c3b"):
+        return StopWorkload(name, 16, 0, False)
+    if name == "c3s":
+        return StopWorkload(name, 20, 0, False)
+    raise SystemExit("unknown workload " + name)
+
+
+# --------------------------------------------------------------------------
+
 def run_reference(args, world, rank):
-    """Reference arm: the oracle port of the reference CPU path, rank 0 only."""
+    """Reference arm: the oracle port of the reference's CPU path, rank 0 only."""
     if rank != 0:
         return
-    from naivesat_b200 import workloads as W
-    from oracle import oracle as O
-    circ = W.config(WORKLOAD)
-    oc = O.Circuit(circ.n, circ.gates, circ.outputs)
+    wl = make_workload(args.workload, args.log2)
     threads = os.cpu_count() or 1
-    # size one step to about 4 s of CPU work
-    bits = 24
-    while True:
-        t0 = time.perf_counter()
-        O.sat_range(oc, 0, 1 << bits, threads)
-        dt = time.perf_counter() - t0
-        if dt > 1.0 or bits >= 34:
-            break
-        bits += 1
-    bits = min(34, bits + max(0, int(round(__import__("math").log2(4.0 / max(dt, 1e-3))))))
-    span = 1 << bits
-    for w in range(args.warmup):
-        O.sat_range(oc, (w % 4) * span % (1 << 36), (w % 4) * span % (1 << 36) + span, threads)
-    times = []
-    for s in range(args.steps):
-        b = (s * span) % (1 << 36)
-        t0 = time.perf_counter()
-        O.sat_range(oc, b, b + span, threads)
-        times.append(time.perf_counter() - t0)
-    tot = sum(times)
-    rate = span * circ.num_gates * args.steps / tot
-    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u64 bit-sliced",
-            "data": "synthetic",
-            "config": {"workload": "naivesat c1: 36-input 3018-gate planted random DAG (seed 1), "
-                                   "bit-sliced exhaustive SAT count + lowest witness",
-                       "inputs": circ.n, "gates": circ.num_gates,
-                       "assignments_per_step": span, "cpu": cpu_model()},
-            "cpu_baseline": {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
-                             "sample": "2^%d assignments per step (of 2^36); the reference's Rust/"
-                                       "gatenative code cannot be built here, so the C restatement in "
-                                       "oracle/ runs it" % bits},
-            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if wl.kind != "sat":
+        vals = [wl.cpu(threads)[0] for _ in range(max(1, args.steps))]
+        rate = statistics.median(vals)
+        sample = "full oracle solve per step"
+        span = None
+    else:
+        from oracle import oracle as O
+        circ = wl.circ
+        oc = O.Circuit(circ.n, circ.gates, circ.outputs)
+        bits = 24
+        while True:
+            t0 = time.perf_counter()
+            O.sat_range(oc, 0, 1 << bits, threads)
+            dt = time.perf_counter() - t0
+            if dt > 1.0 or bits >= min(circ.n, 34):
+                break
+            bits += 1
+        bits = min(min(circ.n, 34), bits + max(0, int(round(math.log2(4.0 / max(dt, 1e-3))))))
+        span = 1 << bits
+        space = 1 << circ.n
+        for w in range(args.warmup):
+            b = (w * span) % space
+            O.sat_range(oc, b, b + span, threads)
+        times = []
+        for s in range(args.steps):
+            b = (s * span) % space
+            t0 = time.perf_counter()
+            O.sat_range(oc, b, b + span, threads)
+            times.append(time.perf_counter() - t0)
+        rate = span * circ.num_gates * args.steps / sum(times)
+        sample = "2^%d assignments per step (of 2^%d)" % (bits, circ.n)
+    line = {"impl": "reference", "metric": wl.metric, "value": rate, "unit": wl.metric, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (1e3 * span * wl.circ.num_gates / rate) if span else None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "u64 bit-sliced", "data": "synthetic",
+            "config": dict(wl.describe(), cpu=cpu_model()),
+            "cpu_baseline": {"value": rate, "unit": wl.metric, "cores": threads, "kind": "port",
+                             "sample": sample + "; the reference's Rust/gatenative code cannot be built "
+                                                "here, so its C restatement in oracle/ runs it"},
+            "e2e": {"value": rate, "unit": wl.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def run_ours(args, world, rank, local):
     import torch
     from naivesat_b200 import api
-    from naivesat_b200 import workloads as W
 
-    circ = W.config(WORKLOAD)
-    n = circ.n
-    total = 1 << min(n, args.log2)
-    per = total // world
-    begin, end = rank * per, (rank + 1) * per
+    wl = make_workload(args.workload, args.log2)
     ctx = api.Context(local)
-    handle = ctx.circuit(circ)
-    live, lop3 = handle.stats()
+    wl.setup(ctx, world, rank)
     torch.cuda.set_device(local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
 
-    def allreduce(vals, op):
+    def reduce(vals, op):
         if world == 1:
             return vals
         import torch.distributed as dist
         t = torch.tensor(vals, dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=op)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
         return t.tolist()
 
     def barrier():
@@ -205,79 +380,75 @@ def run_ours(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # LOP3 issue-rate peak of this GPU (chain microbenchmark)
     peak_lop3, probe_mhz = ctx.lop3_peak()
-    t_jit = time.perf_counter()
-    for w in range(args.warmup):
-        r = handle.sat(find_all=True, begin=begin, end=end)
-    t_jit = time.perf_counter() - t_jit
-    result = r
+    t_warm = time.perf_counter()
+    ref = None
+    for _ in range(args.warmup):
+        ref = wl.step()
+    t_warm = time.perf_counter() - t_warm
 
-    # device-timed steps
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
     dev_ms, launches = [], 0
     for s in range(args.steps):
-        flush.fill_(s)                       # L2 flush between steps (outside the events)
+        flush.fill_(s)                    # L2 flush between steps, outside the events
         torch.cuda.synchronize()
-        r = handle.sat(find_all=True, begin=begin, end=end)
+        r = wl.step()
         dev_ms.append(r["device_ms"])
         launches += r["launches"]
-        assert (r["count"], r["witness"]) == (result["count"], result["witness"])
+        assert ref is None or r["sig"] == ref["sig"], (r["sig"], ref["sig"])
     barrier()
     clk = clocks.stop()
-    # e2e: the C ABI call from host buffers: circuit upload + solve + readback
+
     barrier()
     e2e_ms = []
     for s in range(args.steps):
         t0 = time.perf_counter()
-        h = ctx.circuit(circ)
-        r = h.sat(find_all=True, begin=begin, end=end)
-        del h
+        r = wl.step(fresh=True)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     barrier()
 
-    tot_dev = sum(dev_ms)
-    tot_e2e = sum(e2e_ms)
-    mx = allreduce([tot_dev, tot_e2e], op=__import__("torch.distributed", fromlist=["ReduceOp"]).ReduceOp.MAX
-                   if world > 1 else None)
-    tot_dev, tot_e2e = mx[0], mx[1]
-    cnt = allreduce([float(result["count"])], op=__import__("torch.distributed", fromlist=["ReduceOp"]).ReduceOp.SUM
-                    if world > 1 else None)[0]
+    tot_dev, tot_e2e = reduce([sum(dev_ms), sum(e2e_ms)], "max")
+    extra = {}
+    if wl.kind == "sat":
+        extra["count"] = int(reduce([float(r["count"])], "sum")[0])
+        extra["witness"] = r["witness"]
     if rank != 0:
         return
     steps = args.steps
-    assignments = total * steps
-    value = assignments * circ.num_gates / (tot_dev * 1e-3)
-    e2e = assignments * circ.num_gates / (tot_e2e * 1e-3)
-    # roofline: LOP3 issue.  Algorithmic LOP3 work per 32-lane word = lop3
-    # (LUT-mapped ops of the circuit); per launch-averaged kernel time.
-    words_per_rank = (total // world) // 32
-    lop3_rate = words_per_rank * lop3 * steps / (tot_dev * 1e-3)
-    launches_per_step = launches / steps
+    ms_step = tot_dev / steps
+    value = wl.work() * steps / (tot_dev * 1e-3)
+    e2e = wl.work() * steps / (tot_e2e * 1e-3)
+    lps = launches / steps
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, sample = wl.cpu(threads)
+        if v is not None:
+            cpu = {"value": v, "unit": wl.metric, "cores": threads, "kind": "port",
+                   "sample": sample + ", " + cpu_model()}
+    cfg = wl.describe()
+    cfg.update(extra)
+    if wl.kind != "sat":
+        cfg["result"] = {k: v for k, v in r["result"].items() if k not in ("device_ms", "wall_ms")}
+    cfg["parallelism"] = ("index space split over %d GPU(s)" % world) if wl.kind == "sat" else \
+        "replica per GPU (%d)" % world
+    cfg["l2"] = ("no memory inputs (assignments come from thread indices); " if wl.kind != "stop" else
+                 "table rebuilt every step; ") + "256 MB written between steps to flush L2"
     line = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": tot_dev / steps, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "u32 bit-sliced (lop3.b32)",
-        "data": "synthetic",
-        "config": {"workload": "naivesat c1: 36-input 3018-gate planted random DAG (seed 1), exhaustive "
-                               "SAT over all 2^36 assignments, exact count + lowest witness",
-                   "inputs": n, "gates": circ.num_gates, "live_gates": live, "lop3_per_word": lop3,
-                   "assignments_per_step": total, "parallelism": "index space split over %d GPU(s)" % world,
-                   "l2": "no memory inputs (assignments come from thread indices); 256 MB written "
-                         "between steps to flush L2",
-                   "count": int(cnt), "witness": result["witness"]},
-        "roofline": {"bound": "alu", "achieved": lop3_rate, "peak": peak_lop3, "unit": "lop3/s",
-                     "frac": lop3_rate / peak_lop3, "traffic": None,
-                     "peak_source": "measured lop3.b32 chain microbenchmark on this GPU "
-                                    "(nsat_probe_lop3_peak, %.0f MHz)" % probe_mhz},
-        "cpu_baseline": cpu_baseline(circ) if not args.no_cpu_baseline else None,
-        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": int(32 * launches_per_step),
-                "d2h_bytes_per_step": int(32 * launches_per_step)},
+        "metric": wl.metric, "value": value, "unit": wl.metric, "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "strong" if wl.kind == "sat" else "weak", "vs_baseline": None,
+        "dtype": "u32 bit-sliced (lop3.b32)" if wl.kind != "stop" else "u32/u64 table entries",
+        "data": "synthetic", "config": cfg,
+        "roofline": wl.roofline(world, ms_step, peak_lop3, probe_mhz),
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": wl.metric, "h2d_bytes_per_step": int(32 * lps),
+                "d2h_bytes_per_step": int(32 * lps)},
         "gpu_launches": launches,
         "clocks": clk,
-        "jit_and_warmup_s": t_jit,
+        "warmup_s": t_warm,
     }
     print(json.dumps(line), flush=True)
 
@@ -288,11 +459,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1")
     ap.add_argument("--log2", type=int, default=36,
-                    help="enumerate only the first 2^LOG2 assignments (smaller cases for profiling)")
+                    help="SAT workloads: enumerate only the first 2^LOG2 assignments (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
-    world, rank, local = dist_setup(args)
+    world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)

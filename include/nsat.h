@@ -58,7 +58,8 @@ typedef struct {
     uint32_t no_optimize;     /* 1 = one logic op per gate, no LOP3 cut mapping.
                                  The reference's -n (optimize_negs off) maps here */
     uint32_t verbose;         /* 1 = print JIT/launch details on stderr */
-    uint32_t reserved;
+    uint32_t min_blocks;      /* CTAs per SM the kernels are compiled for
+                                 (__launch_bounds__ minimum); 0 = auto */
 } nsat_opts;
 
 /* ---- context ------------------------------------------------------------ */
@@ -136,7 +137,8 @@ typedef struct {
     int32_t value;             /* truth value of the quantified formula */
     uint64_t solution_lo, solution_hi;  /* bit k = input k of the first block */
     uint32_t launches;
-    uint32_t reserved;
+    uint32_t chunk_bits;       /* log2 assignments per launch actually used */
+    uint64_t scanned;          /* assignments evaluated (launches x 2^chunk_bits) */
     double device_ms;
     double wall_ms;
 } nsat_qsat_result;

@@ -28,7 +28,7 @@ class CircuitDesc(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("no_optimize", C.c_uint32),
-                ("verbose", C.c_uint32), ("reserved", C.c_uint32)]
+                ("verbose", C.c_uint32), ("min_blocks", C.c_uint32)]
 
 
 class SatOpts(C.Structure):
@@ -53,7 +53,7 @@ class QsatResult(C.Structure):
     _fields_ = [("reversed", C.c_int32), ("solution_bits", C.c_uint32),
                 ("has_solution", C.c_int32), ("value", C.c_int32),
                 ("solution_lo", C.c_uint64), ("solution_hi", C.c_uint64),
-                ("launches", C.c_uint32), ("reserved", C.c_uint32),
+                ("launches", C.c_uint32), ("chunk_bits", C.c_uint32), ("scanned", C.c_uint64),
                 ("device_ms", C.c_double), ("wall_ms", C.c_double)]
 
 
@@ -160,10 +160,10 @@ def desc_of(n, gates, outputs):
 class Context:
     """One device + stream; not for concurrent use from several threads."""
 
-    def __init__(self, device=0, block_threads=0, no_optimize=False, verbose=False):
+    def __init__(self, device=0, block_threads=0, no_optimize=False, verbose=False, min_blocks=0):
         L = lib()
         h = C.c_void_p()
-        o = Opts(block_threads, 1 if no_optimize else 0, 1 if verbose else 0, 0)
+        o = Opts(block_threads, 1 if no_optimize else 0, 1 if verbose else 0, min_blocks)
         rc = L.nsat_create(device, C.byref(o), C.byref(h))
         if rc != NSAT_OK:
             raise NsatError("nsat_create(%d): %s" % (device, L.nsat_strerror(rc).decode()))
@@ -213,8 +213,8 @@ class Context:
 def _qsat_dict(r):
     return {"reversed": bool(r.reversed), "solution_bits": r.solution_bits,
             "solution": (r.solution_lo | (r.solution_hi << 64)) if r.has_solution else None,
-            "value": bool(r.value), "launches": r.launches, "device_ms": r.device_ms,
-            "wall_ms": r.wall_ms}
+            "value": bool(r.value), "launches": r.launches, "chunk_bits": r.chunk_bits,
+            "scanned": r.scanned, "device_ms": r.device_ms, "wall_ms": r.wall_ms}
 
 
 class CircuitHandle:

@@ -10,7 +10,7 @@ std::string KernelConfig::key() const {
     std::ostringstream s;
     s << "mode=" << (int)mode << " nin=" << nin << " it=" << it << " wb=" << wb << " cb=" << cb
       << " m=" << m << " q0all=" << q0all << " allbits=" << allbits << " data=" << data
-      << " fmt=" << fmt << " nout=" << nout << " map=";
+      << " fmt=" << fmt << " nout=" << nout << " minb=" << minb << " map=";
     for (int v : in_of_bit) s << v << ',';
     return s.str();
 }
@@ -55,6 +55,8 @@ std::string generate_source(const KernelConfig& kc, const LutNet& net) {
     s << "constexpr int NSAT_NOUT = " << kc.nout << ";\n";
     s << "constexpr int NSAT_NB = " << kc.nb << ";\n";
     s << "constexpr int NSAT_NT = " << kc.threads() << ";\n";
+    if (kc.minb) s << "#define NSAT_BOUNDS __launch_bounds__(" << kc.threads() << ", " << kc.minb << ")\n";
+    else s << "#define NSAT_BOUNDS __launch_bounds__(" << kc.threads() << ")\n";
     s << "constexpr int NSAT_IT = " << kc.it << ";\n";
     s << "constexpr int NSAT_WB = " << kc.wb << ";\n";
     s << "constexpr int NSAT_CB = " << kc.cb << ";\n";

@@ -16,6 +16,7 @@ struct KernelConfig {
     uint32_t nb = 0;           // enumeration bits (== nin)
     std::vector<int> in_of_bit;  // enumeration bit -> circuit input
     uint32_t it = 0, wb = 0, cb = 0;  // log2 iterations/warp, warps/CTA, CTAs/launch
+    uint32_t minb = 0;         // __launch_bounds__ minimum CTAs per SM (0 = none)
     uint32_t c = 0;            // 10 + it + wb + cb
     // QSAT
     uint32_t m = 0;            // unit level (inner bits below the first block)

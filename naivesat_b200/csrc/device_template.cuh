@@ -3,7 +3,8 @@
 // The host generator (codegen.cpp) prepends a prelude that defines:
 //   constexpr ints NSAT_NIN, NSAT_NOUT, NSAT_NB (enumeration bits), NSAT_NT
 //   (threads per CTA), NSAT_IT / NSAT_WB / NSAT_CB (log2 of iterations per
-//   warp, warps per CTA and CTAs per launch), NSAT_C (= 10+IT+WB+CB, log2 of
+//   warp, warps per CTA and CTAs per launch), NSAT_BOUNDS (the kernels'
+//   __launch_bounds__), NSAT_C (= 10+IT+WB+CB, log2 of
 //   assignments per launch), NSAT_M (QSAT unit level), NSAT_Q0ALL,
 //   NSAT_ALLBITS (bit j = quantifier of enumeration bit j is All),
 //   NSAT_DATA (1 = items come from a buffer instead of the circuit),
@@ -48,7 +49,7 @@ __device__ __forceinline__ u64 warp_min_u64(u64 v) {
 #if NSAT_MODE_SAT
 // --------------------------------------------------------------------------
 // SAT: count every satisfying assignment and find the lowest one.
-extern "C" __global__ void __launch_bounds__(NSAT_NT)
+extern "C" __global__ void NSAT_BOUNDS
 nsat_sat(u64 launch, LaunchOut* __restrict__ out) {
     const u32 lane = threadIdx.x & 31u;
     const u32 warp = threadIdx.x >> 5;
@@ -116,7 +117,7 @@ __device__ __forceinline__ u32 decisive(u32 y, int k, int nodes) {
     return (NSAT_Q0ALL ? ~y : y) & unit_mask(k) & valid;
 }
 
-extern "C" __global__ void __launch_bounds__(NSAT_NT)
+extern "C" __global__ void NSAT_BOUNDS
 nsat_qsat(u64 launch, LaunchOut* __restrict__ out, unsigned char* __restrict__ scratch,
           const u32* __restrict__ data) {
     constexpr int M = NSAT_M;
@@ -302,7 +303,7 @@ __device__ __forceinline__ void transpose32(u32* a) {
     }
 }
 
-extern "C" __global__ void __launch_bounds__(NSAT_NT)
+extern "C" __global__ void NSAT_BOUNDS
 nsat_table(u64 nwords, void* __restrict__ table, LaunchOut* __restrict__ out) {
     const u64 stride = (u64)gridDim.x * NSAT_NT;
     u32 anystop = 0;
