@@ -2,7 +2,7 @@
 """Benchmark of the naivesat hot path on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload c1|c0|c1_twin|c2a|c2b|c2c|c3a|c3b|c3s]
+                  [--workload c1|c0|c1_twin|c2a|c2b|c2c|c3a|c3b|c3m|c3s]
 
 Default workload (c1): exhaustive bit-sliced SAT of the 36-input / 3018-gate
 planted random-DAG circuit (seed 1), exact solution count plus lowest witness
@@ -236,6 +236,8 @@ class StopWorkload:
         self.name = name
         if name == "c3s":
             self.circ = W.lfsr_stop(4, 32, 300)
+        elif name == "c3m":
+            self.circ = W.lfsr_stop(4, 28, 300)
         else:
             self.circ = W.config(name)
         self.u, self.mode, self.want_steps = unknowns, mode, steps_counts
@@ -299,7 +301,7 @@ def make_workload(name, log2):
         return QsatWorkload(name)
     if name in ("c3a", "c3b"):
         return StopWorkload(name, 16, 0, False)
-    if name == "c3s":
+    if name in ("c3s", "c3m"):
         return StopWorkload(name, 20, 0, False)
     raise SystemExit("unknown workload " + name)
 
