@@ -127,7 +127,13 @@ int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opts* opts,
  * pushing every circuit value in order into a QuantReducer (qsat.rs:1991). */
 typedef struct {
     uint32_t chunk_bits;   /* log2 assignments per launch (0 = auto) */
-    uint32_t reserved;
+    uint32_t prefix_bits;  /* fix inputs 0..prefix_bits-1 (the outermost
+                              quantifiers) to `prefix` and solve the formula
+                              below them: the result then describes the
+                              sub-formula over inputs prefix_bits..n-1 (its
+                              first block, its value).  Shards of a multi-GPU
+                              solve use this; 0 = the whole formula */
+    uint64_t prefix;       /* input 0 is the most significant of prefix_bits */
 } nsat_qsat_opts;
 
 typedef struct {

@@ -46,7 +46,7 @@ class SatResult(C.Structure):
 
 
 class QsatOpts(C.Structure):
-    _fields_ = [("chunk_bits", C.c_uint32), ("reserved", C.c_uint32)]
+    _fields_ = [("chunk_bits", C.c_uint32), ("prefix_bits", C.c_uint32), ("prefix", C.c_uint64)]
 
 
 class QsatResult(C.Structure):
@@ -247,9 +247,12 @@ class CircuitHandle:
                 "scanned": r.scanned_lo | (r.scanned_hi << 64), "launches": r.launches,
                 "device_ms": r.device_ms, "wall_ms": r.wall_ms}
 
-    def qsat(self, quants, chunk_bits=0):
+    def qsat(self, quants, chunk_bits=0, prefix_bits=0, prefix=0):
+        """QSAT solve; with prefix_bits > 0 the outermost prefix_bits inputs
+        are fixed to `prefix` (input 0 most significant) and the result is
+        that of the sub-formula below them."""
         q = _quants_array(quants, self.n)
-        o = QsatOpts(chunk_bits, 0)
+        o = QsatOpts(chunk_bits, prefix_bits, prefix)
         r = QsatResult()
         self.ctx._check(lib().nsat_qsat_solve(self.ctx.h, self.h, q.ctypes.data_as(U8P), C.byref(o),
                                               C.byref(r)), "qsat_solve")
@@ -259,7 +262,7 @@ class CircuitHandle:
         """nsat_qsat_solve_noalloc: the same solve with no device allocation
         (scratch from the library's static device array)."""
         q = _quants_array(quants, self.n)
-        o = QsatOpts(chunk_bits, 0)
+        o = QsatOpts(chunk_bits, 0, 0)
         r = QsatResult()
         self.ctx._check(lib().nsat_qsat_solve_noalloc(self.ctx.h, self.h, q.ctypes.data_as(U8P), C.byref(o),
                                                       C.byref(r)), "qsat_solve_noalloc")

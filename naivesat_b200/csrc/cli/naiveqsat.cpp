@@ -8,7 +8,12 @@
 // "Result: (Satisfiable)"; <bits> is the first quantifier block, input k at
 // bit k, printed most significant first.  A file that does not parse as a
 // quantified circuit is read as a plain circuit with every input existential
-// (qsat.rs:6277-6285).
+// (qsat.rs:6277-6285).  The combined exec types split the outermost
+// log2(devices) quantifiers over all visible devices, one host thread and
+// context per device, and join the sub-answers with a forall/exists reducer.
+#include <thread>
+
+#include "../qreducer.h"
 #include "cli_common.h"
 
 using namespace cli;
@@ -40,24 +45,66 @@ int main(int argc, char** argv) {
         if (a.has("elem-inputs")) chunk_bits = e;
     }
     ExecType et = parse_exec_type(a.get("exec-type"));
-    printf("Execute in CUDA device=%d\n", et.devices[0]);
-    nsat_ctx* ctx = open_ctx(et.devices[0], a);
-    nsat_circuit* c = nullptr;
-    check(ctx, nsat_circuit_new(ctx, &L.d, &c), "circuit");
-    nsat_qsat_opts o{};
-    o.chunk_bits = chunk_bits;
-    nsat_qsat_result r{};
+    // shard over a power-of-two number of devices on the outermost inputs
+    uint32_t sbits = 0;
+    while ((1u << (sbits + 1)) <= et.devices.size() && sbits + 1 + 14 <= n) sbits++;
+    const size_t D = (size_t)1 << sbits;
+    if (D == 1) printf("Execute in CUDA device=%d\n", et.devices[0]);
+    else printf("Execute in %zu CUDA devices (outermost %u inputs split)\n", D, sbits);
+    std::vector<nsat_qsat_result> subs(D);
+    std::vector<int> rcs(D, 0);
+    std::vector<std::string> errs(D);
     printf("Start execution\n");
     fflush(stdout);
     const double t0 = now_s();
-    check(ctx, nsat_qsat_solve(ctx, c, quants.data(), &o, &r), "qsat solve");
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < D; i++) {
+        th.emplace_back([&, i]() {
+            nsat_ctx* ctx = open_ctx(et.devices[i], a);
+            nsat_circuit* c = nullptr;
+            int rc = nsat_circuit_new(ctx, &L.d, &c);
+            if (rc == NSAT_OK) {
+                nsat_qsat_opts o{};
+                o.chunk_bits = chunk_bits;
+                o.prefix_bits = sbits;
+                o.prefix = i;
+                rc = nsat_qsat_solve(ctx, c, quants.data(), &o, &subs[i]);
+            }
+            rcs[i] = rc;
+            if (rc) errs[i] = nsat_last_error(ctx);
+            nsat_circuit_free(c);
+            nsat_destroy(ctx);
+        });
+    }
+    for (auto& t : th) t.join();
+    for (size_t i = 0; i < D; i++)
+        if (rcs[i]) die(std::string("qsat solve: ") + nsat_strerror(rcs[i]) + " " + errs[i], 1);
+    nsat_qsat_result r = subs[0];
+    if (D > 1) {
+        // forall/exists over the split inputs, sub-answers in prefix order
+        uint32_t f = 0;
+        while (f < n && quants[f] == quants[0]) f++;
+        nsat::QuantReducer qr(std::vector<uint8_t>(quants.begin(), quants.begin() + sbits));
+        nsat::FinalResult fr;
+        for (size_t i = 0; i < D; i++) {
+            const bool value = (subs[i].has_solution != 0) != (subs[i].reversed != 0);
+            qr.push(value);
+            if (!qr.final_result(&fr)) continue;
+            r.reversed = quants[0];
+            r.solution_bits = f;
+            r.has_solution = fr.has_solution;
+            u128 sol = fr.solution;
+            if (fr.has_solution && f > sbits) sol |= ((u128)subs[i].solution_lo) << sbits;
+            r.solution_lo = (uint64_t)sol;
+            r.solution_hi = (uint64_t)(sol >> 64);
+            break;
+        }
+    }
     printf("Time: %.6f\n", now_s() - t0);
     const u128 sol = ((u128)r.solution_hi << 64) | r.solution_lo;
     std::string s;
     if (r.reversed) s = r.has_solution ? "(Unsatisfiable: " + binary(sol, r.solution_bits) + ")" : "(Satisfiable)";
     else s = r.has_solution ? "(Satisfiable: " + binary(sol, r.solution_bits) + ")" : "(Unsatisfiable)";
     printf("Result: %s\n", s.c_str());
-    nsat_circuit_free(c);
-    nsat_destroy(ctx);
     return 0;
 }

@@ -288,24 +288,32 @@ int plan_sat(uint32_t n, const nsat_sat_opts& o, uint32_t block_threads, uint32_
 struct QsatPlan {
     KernelConfig kc;
     std::vector<uint8_t> q;   // padded quantifiers
-    uint32_t n = 0, d = 0, np = 0, f = 0, m = 0, C = 0, A = 0;
+    uint32_t n = 0, d = 0, np = 0, C = 0, A = 0;
+    uint32_t s = 0;           // fixed prefix bits (inputs 0..s-1)
+    uint32_t fsub = 0;        // first quantifier block of the problem below the prefix
+    uint32_t m = 0;           // unit level: np - (s + fsub)
 };
 
 int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint32_t chunk_bits,
-              uint32_t block_threads, uint32_t min_blocks, QsatPlan* pl, std::string* err) {
+              uint32_t block_threads, uint32_t min_blocks, uint32_t prefix_bits, QsatPlan* pl,
+              std::string* err) {
     if (quants_in.size() != n || n == 0) { *err = "quantifier count differs from inputs"; return NSAT_EINVAL; }
+    if (prefix_bits >= n) { *err = "prefix must leave at least one free input"; return NSAT_EINVAL; }
     const uint32_t d = n < 15 ? 15 - n : 0;
     const uint32_t np = n + d;
     if (np > 128) { *err = "too many inputs"; return NSAT_EUNSUPPORTED; }
     std::vector<uint8_t> q = quants_in;
     for (uint32_t k = 0; k < d; k++) q.push_back(quants_in[n - 1] ? 0 : 1);
-    uint32_t f = 0;
-    while (f < n && q[f] == q[0]) f++;
-    const uint32_t m = np - f;
+    const uint32_t s = prefix_bits;
+    uint32_t fsub = 0;
+    while (s + fsub < n && q[s + fsub] == q[s]) fsub++;
+    if (fsub > 64) { *err = "first quantifier block longer than 64"; return NSAT_EUNSUPPORTED; }
+    const uint32_t m = np - (s + fsub);
     uint32_t C = chunk_bits ? std::max<uint32_t>(15, chunk_bits + d) : 34;
-    C = std::min<uint32_t>(C, np);
+    C = std::min<uint32_t>(C, np - s);
+    if (C < 10) { *err = "prefix leaves fewer than 2^10 assignments"; return NSAT_EINVAL; }
     const uint32_t A = np - C;
-    if (A > 64) { *err = "more than 64 quantifiers above one launch"; return NSAT_EUNSUPPORTED; }
+    if (A - s > 64) { *err = "more than 64 quantifiers above one launch"; return NSAT_EUNSUPPORTED; }
     KernelConfig& kc = pl->kc;
     kc.mode = Mode::QSAT;
     kc.data = data;
@@ -319,11 +327,12 @@ int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint
     choose_shape(C, block_threads, &kc);
     kc.minb = min_blocks ? min_blocks : default_min_blocks(kc);
     kc.m = std::min<uint32_t>(m, 127);
-    kc.q0all = q[0] != 0;
+    kc.q0all = q[s] != 0;
     kc.allbits = 0;
     for (uint32_t j = 0; j < std::min<uint32_t>(C, 64); j++)
         if (q[np - 1 - j]) kc.allbits |= 1ull << j;
-    pl->q = q; pl->n = n; pl->d = d; pl->np = np; pl->f = f; pl->m = m; pl->C = C; pl->A = A;
+    pl->q = q; pl->n = n; pl->d = d; pl->np = np; pl->C = C; pl->A = A;
+    pl->s = s; pl->fsub = fsub; pl->m = m;
     return NSAT_OK;
 }
 
@@ -582,7 +591,7 @@ namespace {
 int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quants_in,
                 const uint32_t* data_words, uint32_t n_items_bits, uint32_t chunk_bits,
                 nsat_qsat_result* res, unsigned char* fixed_scratch = nullptr,
-                size_t fixed_scratch_bytes = 0) {
+                size_t fixed_scratch_bytes = 0, uint32_t prefix_bits = 0, uint64_t prefix = 0) {
     memset(res, 0, sizeof(*res));
     const double t_start = now_ms();
     if (int rc = set_device(ctx)) return rc;
@@ -590,11 +599,18 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     const uint32_t n = data ? n_items_bits : c->circ.n;
     QsatPlan plan;
     std::string perr;
-    if (int rc = plan_qsat(n, quants_in, data, chunk_bits, ctx->opts.block_threads, ctx->opts.min_blocks, &plan, &perr))
+    if (int rc = plan_qsat(n, quants_in, data, chunk_bits, ctx->opts.block_threads, ctx->opts.min_blocks,
+                           prefix_bits, &plan, &perr))
         return fail(ctx, rc, perr);
+    if (prefix_bits < 64 && (prefix >> prefix_bits) != 0) return fail(ctx, NSAT_EINVAL, "prefix wider than prefix_bits");
     const KernelConfig& kc = plan.kc;
     const std::vector<uint8_t>& q = plan.q;
-    const uint32_t d = plan.d, np = plan.np, f = plan.f, m = plan.m, C = plan.C, A = plan.A;
+    // below a fixed prefix of s inputs the problem is the sub-formula over
+    // inputs s..n-1: its first block has fsub inputs and As quantifiers lie
+    // above one launch
+    const uint32_t d = plan.d, np = plan.np, m = plan.m, C = plan.C, s = plan.s, f = plan.fsub;
+    const uint32_t A = plan.A - s;
+    const uint64_t L0 = s ? (prefix << A) : 0;
     LutNet empty;
     const std::vector<uint32_t> out0{0};
     const LutNet& net = data ? empty : get_net(c, out0);
@@ -627,10 +643,10 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
         CK(cudaMemcpyAsync(ctx->d_data, ex.data(), nw * 4, cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     }
-    const bool q0all = q[0] != 0;
+    const bool q0all = q[s] != 0;
     const bool dec = !q0all;   // value of a decisive unit
     std::unique_ptr<QuantReducer> qr;
-    if (A > 0) qr.reset(new QuantReducer(std::vector<uint8_t>(q.begin(), q.begin() + A)));
+    if (A > 0) qr.reset(new QuantReducer(std::vector<uint8_t>(q.begin() + s, q.begin() + s + A)));
     FinalResult fr;
     bool have = false;
     uint64_t nl = A == 64 ? ~0ull : (1ull << A);
@@ -644,7 +660,7 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     int rc = run_ring(
         ctx, nl,
         [&](uint64_t k, int slot) {
-            launch_idx_buf[slot] = k;
+            launch_idx_buf[slot] = L0 + k;
             LaunchOut* po = d_out + slot;
             void* params[] = {&launch_idx_buf[slot], &po, &scratch, &dd};
             return launch(ctx, fn, grid, threads, params);
@@ -704,7 +720,8 @@ extern "C" int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* qu
     uint32_t f = 0;
     while (f < q.size() && q[f] == q[0]) f++;
     if (f > 64) return fail(ctx, NSAT_EUNSUPPORTED, "first quantifier block longer than 64");
-    return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res);
+    return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res, nullptr, 0,
+                       opts ? opts->prefix_bits : 0, opts ? opts->prefix : 0);
 }
 
 int nsat::ctx_device(const nsat_ctx* ctx) { return ctx ? ctx->device : -1; }
@@ -718,7 +735,8 @@ int nsat::qsat_solve_with_scratch(nsat_ctx* ctx, nsat_circuit* c, const uint8_t*
     uint32_t f = 0;
     while (f < q.size() && q[f] == q[0]) f++;
     if (f > 64) return fail(ctx, NSAT_EUNSUPPORTED, "first quantifier block longer than 64");
-    return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res, scratch, scratch_bytes);
+    return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res, scratch, scratch_bytes,
+                       opts ? opts->prefix_bits : 0, opts ? opts->prefix : 0);
 }
 
 extern "C" int nsat_qsat_reduce_words(nsat_ctx* ctx, const uint8_t* quants, uint32_t nq,
@@ -931,7 +949,7 @@ extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quan
         std::vector<uint8_t> q(quants, quants + c.n);
         for (auto& v : q) v = v ? 1 : 0;
         QsatPlan pl;
-        rc = plan_qsat(c.n, q, false, 0, bt, mb, &pl, &err);
+        rc = plan_qsat(c.n, q, false, 0, bt, mb, 0, &pl, &err);
         kc = pl.kc;
     } else {
         rc = plan_table(c, false, &kc, &err);

@@ -20,3 +20,10 @@ def ctx():
     c = api.Context(0)
     yield c
     c.close()
+
+
+# test modules import helpers from one another (e.g. test_gpu_shard uses
+# test_shard.oracle_sub)
+TESTS = os.path.dirname(os.path.abspath(__file__))
+if TESTS not in sys.path:
+    sys.path.insert(0, TESTS)
