@@ -213,6 +213,89 @@ typedef struct {
 int nsat_stop_solve(nsat_ctx* ctx, nsat_table* t, const nsat_stop_opts* opts,
                     nsat_stop_result* res);
 
+/* ---- batched serving ---------------------------------------------------- */
+/* A server runs many SAT / QSAT / SATOSTOP jobs on one device concurrently
+ * (no counterpart in the reference, which solves one circuit per process).
+ * Circuits are interpreted as LUT bytecode by one precompiled kernel, so a
+ * new circuit costs no compilation; jobs are admitted in arrival order while
+ * their device memory fits the server's budget; every nsat_server_step runs
+ * one epoch (one CUDA-graph replay) over a slice of tiles (2^15 assignments)
+ * of every active job, slices doubling from one tile, and retires finished
+ * jobs.  Answers equal the one-shot solvers': SAT the lowest witness, QSAT
+ * the QuantReducer result, SATOSTOP the lowest stopping start with steps. */
+typedef struct nsat_server nsat_server;
+
+typedef struct {
+    uint64_t arena_bytes;       /* device memory for admitted jobs; 0 = 1 GiB */
+    uint32_t max_active;        /* jobs sharing the device at once (<= 512); 0 = 512 */
+    uint32_t max_queue;         /* waiting jobs before submit returns NSAT_EBUSY; 0 = 2^20 */
+    uint32_t max_slice_tiles;   /* cap of one job's tiles per epoch; 0 = 4096 */
+    uint32_t first_slice_tiles; /* a new job's first slice (doubling after); 0 = 1 */
+    uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = 1.2e7 */
+} nsat_server_opts;
+
+typedef struct {
+    uint32_t kind;              /* 0 = SAT, 1 = QSAT, 2 = SATOSTOP */
+    uint32_t unknowns;          /* SATOSTOP: the top `unknowns` state bits */
+    const uint8_t* quants;      /* QSAT: one per input, 1 = All */
+    nsat_circuit_desc circuit;
+    uint64_t tag;               /* returned with the result */
+} nsat_job_desc;
+
+typedef struct {
+    uint64_t id, tag;
+    int32_t status;
+    uint32_t kind;
+    int32_t satisfiable;        /* SAT */
+    int32_t value;              /* QSAT: truth value */
+    uint64_t witness_lo, witness_hi;   /* SAT: lowest satisfying index */
+    uint64_t count;             /* SAT: solutions in the evaluated tiles */
+    int32_t reversed;           /* QSAT FinalResult */
+    uint32_t solution_bits;
+    int32_t has_solution;
+    int32_t found;              /* SATOSTOP */
+    uint64_t solution;
+    uint64_t start, end, steps; /* SATOSTOP */
+    uint64_t tiles;             /* tiles evaluated */
+    double submit_ms, admit_ms, done_ms;   /* steady clock, milliseconds */
+} nsat_job_result;
+
+typedef struct {
+    uint64_t epochs;
+    double device_ms;           /* interpreter kernel time, CUDA events */
+    uint32_t active, queued;
+    uint64_t arena_used, arena_bytes;
+    uint32_t graph_slots, grid;
+} nsat_server_stats_t;
+
+int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out);
+void nsat_server_destroy(nsat_server* s);
+/* Queues a job (the circuit is copied); NSAT_EBUSY when the queue is full. */
+int nsat_server_submit(nsat_server* s, const nsat_job_desc* job, uint64_t* id);
+/* Admits what fits and runs one epoch; reports jobs still active / queued. */
+int nsat_server_step(nsat_server* s, uint32_t* active, uint32_t* queued);
+/* Moves up to `cap` finished results to `out`. */
+int nsat_server_poll(nsat_server* s, nsat_job_result* out, uint32_t cap, uint32_t* n);
+int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st);
+
+/* ---- seeded benchmark circuits ------------------------------------------- */
+/* Random DAG of the benchmark configurations: `gates` two-input gates, types
+ * uniform over the four, each fan-in uniform over the preceding `window`
+ * wires and negated with probability 1/4 (negations folded into the gate
+ * functions); the single output is the last gate, or with live_output the last
+ * gate that is not constant on 4096 seeded samples.  splitmix64(seed) drives
+ * every draw.  Writes up to gate_cap gates / out_cap outputs; returns the
+ * counts. */
+int nsat_gen_random_dag(uint64_t seed, uint32_t n, uint32_t gates, uint32_t window, int live_output,
+                        uint32_t* out_gates, uint32_t gate_cap, uint32_t* out_outputs, uint32_t out_cap,
+                        uint32_t* gate_num, uint32_t* out_num);
+/* SATOSTOP next-state circuit: n-bit Fibonacci LFSR (4 seeded taps, n-1
+ * among them) XOR the last n gates of a seeded `mixer_gates`-gate random DAG;
+ * STOP = (state == seeded pattern).  n+1 outputs. */
+int nsat_gen_lfsr_stop(uint64_t seed, uint32_t n, uint32_t mixer_gates, uint32_t* out_gates,
+                       uint32_t gate_cap, uint32_t* out_outputs, uint32_t out_cap, uint32_t* gate_num,
+                       uint32_t* out_num, uint64_t* pattern);
+
 /* ---- build check -------------------------------------------------------- */
 /* Generates and NVRTC-compiles for sm_100a, without a device, the kernel that
  * a solve of `kind` (0 = SAT, 1 = QSAT, 2 = SATOSTOP table) would launch for

@@ -76,13 +76,42 @@ class StopResult(C.Structure):
                 ("join_ms", C.c_double)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("arena_bytes", C.c_uint64), ("max_active", C.c_uint32), ("max_queue", C.c_uint32),
+                ("max_slice_tiles", C.c_uint32), ("first_slice_tiles", C.c_uint32),
+                ("epoch_budget", C.c_uint64)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("unknowns", C.c_uint32), ("quants", U8P),
+                ("circuit", CircuitDesc), ("tag", C.c_uint64)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("tag", C.c_uint64), ("status", C.c_int32), ("kind", C.c_uint32),
+                ("satisfiable", C.c_int32), ("value", C.c_int32), ("witness_lo", C.c_uint64),
+                ("witness_hi", C.c_uint64), ("count", C.c_uint64), ("reversed", C.c_int32),
+                ("solution_bits", C.c_uint32), ("has_solution", C.c_int32), ("found", C.c_int32),
+                ("solution", C.c_uint64), ("start", C.c_uint64), ("end", C.c_uint64), ("steps", C.c_uint64),
+                ("tiles", C.c_uint64), ("submit_ms", C.c_double), ("admit_ms", C.c_double),
+                ("done_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("epochs", C.c_uint64), ("device_ms", C.c_double), ("active", C.c_uint32),
+                ("queued", C.c_uint32), ("arena_used", C.c_uint64), ("arena_bytes", C.c_uint64),
+                ("graph_slots", C.c_uint32), ("grid", C.c_uint32)]
+
+
 EXPORTS = [
     "nsat_create", "nsat_destroy", "nsat_strerror", "nsat_last_error", "nsat_device_count",
     "nsat_circuit_new", "nsat_circuit_free", "nsat_circuit_stats", "nsat_parse",
     "nsat_parsed_get", "nsat_parsed_free", "nsat_format", "nsat_sat_solve", "nsat_qsat_solve",
     "nsat_qsat_reduce_words", "nsat_stop_table_build", "nsat_table_free", "nsat_table_read",
     "nsat_table_bytes", "nsat_stop_solve", "nsat_probe_lop3_peak", "nsat_jit_check",
-    "nsat_qsat_solve_noalloc",
+    "nsat_qsat_solve_noalloc", "nsat_server_create", "nsat_server_destroy", "nsat_server_submit",
+    "nsat_server_step", "nsat_server_poll", "nsat_server_stats", "nsat_gen_random_dag",
+    "nsat_gen_lfsr_stop",
 ]
 
 _lib = None
@@ -129,6 +158,17 @@ def lib():
         L.nsat_table_bytes.restype = C.c_uint64
         L.nsat_stop_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(StopOpts), C.POINTER(StopResult)]
         L.nsat_probe_lop3_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.nsat_server_create.argtypes = [C.c_void_p, C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]
+        L.nsat_server_destroy.argtypes = [C.c_void_p]
+        L.nsat_server_destroy.restype = None
+        L.nsat_server_submit.argtypes = [C.c_void_p, C.POINTER(JobDesc), C.POINTER(C.c_uint64)]
+        L.nsat_server_step.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.nsat_server_poll.argtypes = [C.c_void_p, C.POINTER(JobResult), C.c_uint32, C.POINTER(C.c_uint32)]
+        L.nsat_server_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.nsat_gen_random_dag.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, U32P,
+                                          C.c_uint32, U32P, C.c_uint32, U32P, U32P]
+        L.nsat_gen_lfsr_stop.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, U32P, C.c_uint32, U32P,
+                                         C.c_uint32, U32P, U32P, U64P]
         L.nsat_jit_check.argtypes = [C.POINTER(CircuitDesc), U8P, C.c_int, C.POINTER(Opts),
                                      C.POINTER(JitInfo), C.c_char_p, C.c_size_t]
         _lib = L
@@ -272,6 +312,82 @@ class CircuitHandle:
         return Table(self, want_steps)
 
 
+KINDS = {"sat": 0, "qsat": 1, "stop": 2}
+
+
+class Server:
+    """Batched serving of many SAT / QSAT / SATOSTOP jobs on one context."""
+
+    def __init__(self, ctx, arena_bytes=0, max_active=0, max_queue=0, max_slice_tiles=0,
+                 first_slice_tiles=0, epoch_budget=0):
+        self.ctx = ctx
+        o = ServerOpts(arena_bytes, max_active, max_queue, max_slice_tiles, first_slice_tiles, epoch_budget)
+        h = C.c_void_p()
+        ctx._check(lib().nsat_server_create(ctx.h, C.byref(o), C.byref(h)), "server_create")
+        self.h = h
+        self._buf = (JobResult * 256)()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nsat_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, kind, circ, quants=None, unknowns=0, tag=0):
+        """kind: 'sat' | 'qsat' | 'stop'.  Returns the job id (raises NsatError
+        with EBUSY when the queue is full)."""
+        d = desc_of(circ.n, circ.gates, circ.outputs)
+        q = _quants_array(quants, circ.n) if quants is not None else None
+        jd = JobDesc(KINDS[kind], unknowns, q.ctypes.data_as(U8P) if q is not None else None, d, tag)
+        jid = C.c_uint64()
+        self.ctx._check(lib().nsat_server_submit(self.h, C.byref(jd), C.byref(jid)), "server_submit")
+        return jid.value
+
+    def step(self):
+        a, q = C.c_uint32(), C.c_uint32()
+        self.ctx._check(lib().nsat_server_step(self.h, C.byref(a), C.byref(q)), "server_step")
+        return a.value, q.value
+
+    def poll(self):
+        out = []
+        while True:
+            n = C.c_uint32()
+            self.ctx._check(lib().nsat_server_poll(self.h, self._buf, len(self._buf), C.byref(n)), "server_poll")
+            for i in range(n.value):
+                r = self._buf[i]
+                d = {"id": r.id, "tag": r.tag, "kind": ["sat", "qsat", "stop"][r.kind], "tiles": r.tiles,
+                     "submit_ms": r.submit_ms, "admit_ms": r.admit_ms, "done_ms": r.done_ms}
+                if r.kind == 0:
+                    d.update(satisfiable=bool(r.satisfiable), count=r.count,
+                             witness=(r.witness_lo | (r.witness_hi << 64)) if r.satisfiable else None)
+                elif r.kind == 1:
+                    d.update(reversed=bool(r.reversed), solution_bits=r.solution_bits, value=bool(r.value),
+                             solution=r.solution if r.has_solution else None)
+                else:
+                    d.update(found=bool(r.found), start=r.start if r.found else None,
+                             end=r.end if r.found else None, steps=r.steps if r.found else None)
+                out.append(d)
+            if n.value < len(self._buf):
+                return out
+
+    def stats(self):
+        st = ServerStats()
+        self.ctx._check(lib().nsat_server_stats(self.h, C.byref(st)), "server_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def run_all(self, max_steps=10_000_000):
+        """Steps until every submitted job finished; returns the results."""
+        res = []
+        for _ in range(max_steps):
+            a, q = self.step()
+            res += self.poll()
+            if a == 0 and q == 0:
+                return res
+        raise NsatError("server did not drain in %d steps" % max_steps)
+
+
 class Table:
     def __init__(self, circ, want_steps=False):
         self.ctx = circ.ctx
@@ -365,6 +481,31 @@ def jit_check(circ, kind="sat", quants=None, block_threads=0, no_optimize=False)
     return {"regs": info.regs, "spill_bytes": info.spill_bytes, "lop3_ops": info.lop3_ops,
             "live_gates": info.live_gates, "compile_ms": info.compile_ms,
             "log": buf.value.decode(errors="replace")}
+
+
+def gen_random_dag(seed, n, gates, window=64, live_output=False):
+    """nsat_gen_random_dag -> (gates (g,3), outputs (1,2))."""
+    g = np.zeros(3 * gates, dtype=np.uint32)
+    o = np.zeros(2, dtype=np.uint32)
+    gn, on = C.c_uint32(), C.c_uint32()
+    rc = lib().nsat_gen_random_dag(seed, n, gates, window, 1 if live_output else 0, g.ctypes.data_as(U32P),
+                                   gates, o.ctypes.data_as(U32P), 1, C.byref(gn), C.byref(on))
+    if rc != NSAT_OK:
+        raise NsatError("gen_random_dag: %s" % ERRORS.get(rc, rc))
+    return g.reshape(-1, 3), o.reshape(-1, 2)
+
+
+def gen_lfsr_stop(seed, n, mixer_gates):
+    """nsat_gen_lfsr_stop -> (gates, outputs, pattern)."""
+    cap = mixer_gates + 2 * n + 8
+    g = np.zeros(3 * cap, dtype=np.uint32)
+    o = np.zeros(2 * (n + 1), dtype=np.uint32)
+    gn, on, pat = C.c_uint32(), C.c_uint32(), C.c_uint64()
+    rc = lib().nsat_gen_lfsr_stop(seed, n, mixer_gates, g.ctypes.data_as(U32P), cap, o.ctypes.data_as(U32P),
+                                  n + 1, C.byref(gn), C.byref(on), C.byref(pat))
+    if rc != NSAT_OK:
+        raise NsatError("gen_lfsr_stop: %s" % ERRORS.get(rc, rc))
+    return g[:3 * gn.value].reshape(-1, 3), o.reshape(-1, 2), pat.value
 
 
 def device_count():

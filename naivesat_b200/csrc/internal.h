@@ -3,12 +3,26 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "nsat.h"
+
+#include <cuda_runtime.h>
+
+#include "circuit.h"
 
 namespace nsat {
 
-// Device ordinal a context is bound to.
+// Device ordinal a context is bound to, its stream and SM count.
 int ctx_device(const nsat_ctx* ctx);
+cudaStream_t ctx_stream(const nsat_ctx* ctx);
+int ctx_sm_count(const nsat_ctx* ctx);
+bool ctx_no_optimize(const nsat_ctx* ctx);
+// Records a failure on the context (nsat_last_error) and returns `code`.
+int ctx_fail(nsat_ctx* ctx, int code, const std::string& msg);
+
+// Circuit from the C ABI's flat description (not validated).
+Circuit circuit_from_desc(const nsat_circuit_desc* d);
 
 // nsat_qsat_solve with the last-CTA scratch area supplied by the caller
 // instead of the context's cudaMalloc'd buffer; fails with NSAT_EUNSUPPORTED

@@ -174,6 +174,10 @@ int jit_get(int device, const std::string& src, const std::vector<std::string>& 
     auto m = std::make_shared<JitModule>();
     char name[64];
     snprintf(name, sizeof(name), "%016llx", (unsigned long long)key);
+    if (const char* dump = getenv("NSAT_DUMP_DIR")) {   // generated CUDA source, for inspection
+        mkdirs(dump);
+        write_file_atomic(std::string(dump) + "/" + name + ".cu", src);
+    }
     const std::string dir = cache_dir();
     const std::string cubin_path = dir + "/" + name + ".cubin";
     std::string cubin;

@@ -725,6 +725,11 @@ extern "C" int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* qu
 }
 
 int nsat::ctx_device(const nsat_ctx* ctx) { return ctx ? ctx->device : -1; }
+cudaStream_t nsat::ctx_stream(const nsat_ctx* ctx) { return ctx->stream; }
+int nsat::ctx_sm_count(const nsat_ctx* ctx) { return ctx->sm_count; }
+bool nsat::ctx_no_optimize(const nsat_ctx* ctx) { return ctx->opts.no_optimize != 0; }
+int nsat::ctx_fail(nsat_ctx* ctx, int code, const std::string& msg) { return fail(ctx, code, msg); }
+Circuit nsat::circuit_from_desc(const nsat_circuit_desc* d) { return from_desc(d); }
 
 int nsat::qsat_solve_with_scratch(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
                                    const nsat_qsat_opts* opts, nsat_qsat_result* res,
@@ -961,6 +966,10 @@ extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quan
     info->lop3_ops = (uint32_t)net.luts.size();
     info->live_gates = net.live_gates;
     std::string src = generate_source(kc, net);
+    if (const char* dump = getenv("NSAT_DUMP_DIR")) {   // generated CUDA source, for inspection
+        FILE* f = fopen((std::string(dump) + "/jit_check_kind" + std::to_string(kind) + ".cu").c_str(), "w");
+        if (f) { fwrite(src.data(), 1, src.size(), f); fclose(f); }
+    }
     std::string clog;
     double ms = 0;
     rc = jit_compile_only(src, &clog, &ms, &err);

@@ -1,0 +1,579 @@
+// serve.cpp -- batched serving of SAT / QSAT / SATOSTOP jobs on one device.
+//
+// Jobs are admitted by device memory (a first-fit arena of the server's
+// budget), their circuits become LUT bytecode (no compilation), and every
+// epoch one CUDA graph runs the interpreter kernel over a slice of tiles of
+// every active job: H2D of the epoch's job table, the kernel, D2H of the
+// results.  Slices start at one tile (cheap early exits) and double per
+// epoch up to a cap, so new arrivals share the device with long jobs right
+// away.  Completion rules follow the one-shot solvers:
+//   SAT    lowest witness (all lower tiles were evaluated in earlier epochs);
+//   QSAT   lowest decisive unit inside tiles, or a host forall/exists reducer
+//          over per-tile values for quantifiers above the tile;
+//   TABLE  next-state table built tile by tile, then synchronous doubling
+//          with step counts (naivesatostop semantics, lowest stopping start).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "circuit.h"
+#include "internal.h"
+#include "lutmap.h"
+#include "nsat.h"
+#include "qreducer.h"
+#include "serve_common.h"
+#include "serve_kernels.h"
+#include "static_kernels.h"
+
+using namespace nsat;
+
+namespace {
+
+constexpr uint32_t kMaxActive = 512;
+constexpr size_t kValsCap = 256 * 1024;      // QSAT tile values per epoch
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+uint64_t reverse_bits(uint64_t v, uint32_t bits) {
+    uint64_t r = 0;
+    for (uint32_t k = 0; k < bits; k++) r |= ((v >> k) & 1ull) << (bits - 1 - k);
+    return r;
+}
+
+// First-fit allocator over one device allocation (offsets, 256-byte aligned).
+struct Arena {
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+    std::map<size_t, size_t> free_;   // offset -> size
+    bool alloc(size_t bytes, size_t* off) {
+        bytes = (bytes + 255) & ~(size_t)255;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                *off = it->first;
+                size_t rest = it->second - bytes;
+                size_t noff = it->first + bytes;
+                free_.erase(it);
+                if (rest) free_[noff] = rest;
+                used += bytes;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes) {
+        bytes = (bytes + 255) & ~(size_t)255;
+        used -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) { it->second += nx->second; free_.erase(nx); }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) { pv->second += it->second; free_.erase(it); }
+        }
+    }
+};
+
+// LUT cover of the requested outputs, slot-allocated: inputs keep slots
+// 0..n-1 for the whole tile, gate values reuse slots after their last use.
+struct Program {
+    std::vector<uint64_t> ins;
+    std::vector<uint16_t> outs;
+    uint32_t nslots = 0;
+};
+
+bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool raw, Program* p, std::string* err) {
+    LutNet net = map_luts(c, which, raw);
+    const uint32_t W = c.wires();
+    std::vector<int64_t> last(W, -1);
+    for (size_t k = 0; k < net.luts.size(); k++)
+        for (int i = 0; i < 3; i++) last[net.luts[k].in[i]] = (int64_t)k;
+    for (const Output& o : net.outs) last[o.wire] = INT64_MAX;
+    std::vector<int32_t> slot(W, -1);
+    for (uint32_t i = 0; i < c.n; i++) slot[i] = (int32_t)i;
+    uint32_t next = c.n;
+    std::vector<uint32_t> freel;
+    p->ins.clear();
+    for (size_t k = 0; k < net.luts.size(); k++) {
+        const Lut& L = net.luts[k];
+        uint32_t d;
+        if (!freel.empty()) { d = freel.back(); freel.pop_back(); }
+        else d = next++;
+        slot[L.wire] = (int32_t)d;
+        p->ins.push_back((uint64_t)slot[L.in[0]] | ((uint64_t)slot[L.in[1]] << 12) | ((uint64_t)slot[L.in[2]] << 24) |
+                         ((uint64_t)d << 36) | ((uint64_t)L.tt << 48));
+        // free gate slots whose last use is this LUT (after the write: no aliasing)
+        for (int i = 0; i < 3; i++) {
+            const uint32_t w = L.in[i];
+            if (w >= c.n && last[w] == (int64_t)k) {
+                bool dup = false;
+                for (int j = 0; j < i; j++) dup |= (L.in[j] == w);
+                if (!dup) freel.push_back((uint32_t)slot[w]);
+            }
+        }
+    }
+    p->nslots = next;
+    if (next > SRV_MAX_SLOTS) {
+        *err = "circuit needs " + std::to_string(next) + " slots, the interpreter holds " +
+               std::to_string(SRV_MAX_SLOTS);
+        return false;
+    }
+    p->outs.clear();
+    for (const Output& o : net.outs) p->outs.push_back((uint16_t)(slot[o.wire] | (o.neg ? 0x8000 : 0)));
+    return true;
+}
+
+struct Job {
+    uint64_t id = 0, tag = 0;
+    uint32_t kind = 0;
+    Circuit circ;
+    std::vector<uint8_t> quants;
+    uint32_t unknowns = 0;
+    Program prog;
+    uint32_t n = 0, nb = 0, d = 0;   // inputs, enumeration bits, dummy bits
+    uint32_t f = 0, m = 0;           // QSAT first block length, unit level
+    uint64_t total_tiles = 0, cursor = 0, slice = 1;
+    std::unique_ptr<QuantReducer> qr;
+    SrvJob rec{};
+    size_t prog_off = 0, outs_off = 0, table_off = 0, table2_off = 0, reserve = 0;
+    bool any_stop = false;
+    bool finished = false;
+    uint64_t count = 0;
+    nsat_job_result res{};
+};
+
+}  // namespace
+
+struct nsat_server {
+    nsat_ctx* ctx = nullptr;
+    nsat_server_opts opts{};
+    Arena arena;
+    std::deque<std::unique_ptr<Job>> queue;
+    std::vector<std::unique_ptr<Job>> active;
+    std::vector<nsat_job_result> done;
+    uint64_t next_id = 1;
+    uint32_t rr = 0;   // rotating start of the epoch table
+    SrvEpoch* d_hdr = nullptr;
+    SrvJob* d_jobs = nullptr;
+    uint8_t* d_vals = nullptr;
+    SrvEpoch* h_hdr = nullptr;
+    SrvJob* h_jobs = nullptr;
+    uint8_t* h_vals = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    uint32_t graph_slots = 0;
+    int grid = 0;
+    NsatJoinState* d_join = nullptr;
+    NsatJoinState* h_join = nullptr;
+    uint64_t epochs = 0;
+    double device_ms = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    ~nsat_server() {
+        cudaSetDevice(ctx_device(ctx));
+        cudaStreamSynchronize(ctx_stream(ctx));
+        if (graph) cudaGraphExecDestroy(graph);
+        cudaFree(arena.base);
+        cudaFree(d_hdr);
+        cudaFree(d_jobs);
+        cudaFree(d_vals);
+        cudaFree(d_join);
+        cudaFreeHost(h_hdr);
+        cudaFreeHost(h_jobs);
+        cudaFreeHost(h_vals);
+        cudaFreeHost(h_join);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace {
+
+#define SCK(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return ctx_fail(s->ctx, e_ == cudaErrorMemoryAllocation ? NSAT_ENOMEM : NSAT_ECUDA,      \
+                            std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+    } while (0)
+
+int capture_graph(nsat_server* s, uint32_t slots) {
+    cudaStream_t st = ctx_stream(s->ctx);
+    int per_sm = 0;
+    if (nsat_serve_occupancy(slots, &per_sm) || per_sm < 1)
+        return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, "interpreter does not fit with " + std::to_string(slots) + " slots");
+    s->grid = per_sm * ctx_sm_count(s->ctx);
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    SCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(s->d_hdr, s->h_hdr, sizeof(SrvEpoch), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s->d_jobs, s->h_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyHostToDevice, st);
+    cudaEventRecord(s->ev0, st);
+    int rc = nsat_launch_serve_epoch(s->d_hdr, s->d_jobs, slots, s->d_vals, s->grid, st);
+    cudaEventRecord(s->ev1, st);
+    cudaMemcpyAsync(s->h_jobs, s->d_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(s->h_vals, s->d_vals, kValsCap, cudaMemcpyDeviceToHost, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (rc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return ctx_fail(s->ctx, NSAT_ECUDA, "epoch graph capture failed");
+    }
+    cudaError_t ie = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return ctx_fail(s->ctx, NSAT_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+    s->graph_slots = slots;
+    return NSAT_OK;
+}
+
+void finish(nsat_server* s, Job* j) {
+    j->res.done_ms = now_ms();
+    j->res.status = NSAT_OK;
+    s->done.push_back(j->res);
+}
+
+int admit(nsat_server* s, Job* j) {
+    const size_t pbytes = j->prog.ins.size() * 8 + 8, obytes = j->prog.outs.size() * 2 + 2;
+    size_t tbytes = j->kind == SRV_TABLE ? ((size_t)8 << j->n) : 0;
+    if (!s->arena.alloc(pbytes, &j->prog_off)) return 1;
+    if (!s->arena.alloc(obytes, &j->outs_off)) { s->arena.release(j->prog_off, pbytes); return 1; }
+    if (tbytes) {
+        if (!s->arena.alloc(tbytes, &j->table_off)) {
+            s->arena.release(j->prog_off, pbytes); s->arena.release(j->outs_off, obytes); return 1;
+        }
+        if (!s->arena.alloc(tbytes, &j->table2_off)) {
+            s->arena.release(j->prog_off, pbytes); s->arena.release(j->outs_off, obytes);
+            s->arena.release(j->table_off, tbytes); return 1;
+        }
+    }
+    j->reserve = pbytes + obytes + 2 * tbytes;
+    cudaStream_t st = ctx_stream(s->ctx);
+    SCK(cudaMemcpyAsync(s->arena.base + j->prog_off, j->prog.ins.data(), j->prog.ins.size() * 8, cudaMemcpyHostToDevice, st));
+    SCK(cudaMemcpyAsync(s->arena.base + j->outs_off, j->prog.outs.data(), j->prog.outs.size() * 2, cudaMemcpyHostToDevice, st));
+    SrvJob& r = j->rec;
+    memset(&r, 0, sizeof(r));
+    r.prog = (const srv_u64*)(s->arena.base + j->prog_off);
+    r.outs = (const uint16_t*)(s->arena.base + j->outs_off);
+    r.table = tbytes ? (srv_u64*)(s->arena.base + j->table_off) : nullptr;
+    r.ninstr = (uint32_t)j->prog.ins.size();
+    r.nslots = j->prog.nslots;
+    r.kind = j->kind;
+    r.nb = j->nb;
+    r.nout = (uint32_t)j->prog.outs.size();
+    r.m = j->m;
+    r.n = j->n;
+    for (int p = 0; p < SRV_MAX_NB; p++) r.in_slot[p] = -1;
+    if (j->kind == SRV_SAT) {
+        for (uint32_t p = j->d; p < j->nb; p++) r.in_slot[p] = (int8_t)(p - j->d);
+    } else if (j->kind == SRV_QSAT) {
+        for (uint32_t p = 0; p < j->nb; p++) {
+            int in = (int)(j->nb - 1 - p);
+            if (in < (int)j->n) r.in_slot[p] = (int8_t)in;
+        }
+        r.q0all = j->quants[0];
+        uint64_t ab = 0;
+        for (uint32_t p = 0; p < j->nb && p < 64; p++)
+            if (j->quants[j->nb - 1 - p]) ab |= 1ull << p;
+        r.allbits = ab;
+    } else {
+        for (uint32_t p = 0; p < j->n; p++) r.in_slot[p] = (int8_t)p;
+    }
+    j->res.admit_ms = now_ms();
+    return 0;
+}
+
+void release(nsat_server* s, Job* j) {
+    const size_t pbytes = j->prog.ins.size() * 8 + 8, obytes = j->prog.outs.size() * 2 + 2;
+    s->arena.release(j->prog_off, pbytes);
+    s->arena.release(j->outs_off, obytes);
+    if (j->kind == SRV_TABLE) {
+        const size_t tbytes = (size_t)8 << j->n;
+        s->arena.release(j->table_off, tbytes);
+        s->arena.release(j->table2_off, tbytes);
+    }
+}
+
+// Synchronous doubling on a finished table (naivesatostop: lowest stopping
+// start, with steps).
+int run_joins(nsat_server* s, Job* j) {
+    cudaStream_t st = ctx_stream(s->ctx);
+    j->res.found = 0;
+    if (!j->any_stop) return NSAT_OK;
+    NsatJoinState* h = s->h_join;
+    memset(h, 0, sizeof(*h));
+    for (int i = 0; i < 72; i++) h->best[i] = ~0ull;
+    SCK(cudaMemcpyAsync(s->d_join, h, sizeof(*h), cudaMemcpyHostToDevice, st));
+    void* buf[2] = {s->arena.base + j->table_off, s->arena.base + j->table2_off};
+    int src = 0;
+    for (uint32_t r = 1; r <= j->n; r++) {
+        if (nsat_launch_join_round(2, buf[src], buf[src ^ 1], 1ull << j->n, j->n, j->unknowns, r, 1, s->d_join,
+                                   ctx_sm_count(s->ctx), st))
+            return ctx_fail(s->ctx, NSAT_ECUDA, "join launch failed");
+        src ^= 1;
+    }
+    SCK(cudaMemcpyAsync(h, s->d_join, sizeof(*h), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    const uint32_t fr = h->final_round ? h->final_round : j->n;
+    const uint64_t best = h->best[fr];
+    if (best != ~0ull) {
+        uint64_t e = 0;
+        SCK(cudaMemcpy(&e, (uint64_t*)buf[fr & 1] + best, 8, cudaMemcpyDeviceToHost));
+        j->res.found = 1;
+        j->res.start = best;
+        j->res.end = e & ((1ull << j->n) - 1);
+        j->res.steps = e >> 32;
+    }
+    return NSAT_OK;
+}
+
+}  // namespace
+
+extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out) {
+    if (!ctx || !out) return NSAT_EINVAL;
+    *out = nullptr;
+    std::unique_ptr<nsat_server> sp(new nsat_server());
+    nsat_server* s = sp.get();
+    s->ctx = ctx;
+    if (opts) s->opts = *opts;
+    if (!s->opts.arena_bytes) s->opts.arena_bytes = 1ull << 30;
+    if (!s->opts.max_active || s->opts.max_active > kMaxActive) s->opts.max_active = kMaxActive;
+    if (!s->opts.max_queue) s->opts.max_queue = 1u << 20;
+    if (!s->opts.max_slice_tiles) s->opts.max_slice_tiles = 4096;
+    if (!s->opts.first_slice_tiles) s->opts.first_slice_tiles = 1;
+    if (!s->opts.epoch_budget) s->opts.epoch_budget = 12000000;
+    SCK(cudaSetDevice(ctx_device(ctx)));
+    SCK(cudaMalloc(&s->arena.base, s->opts.arena_bytes));
+    s->arena.cap = s->opts.arena_bytes;
+    s->arena.free_[0] = s->opts.arena_bytes;
+    SCK(cudaMalloc(&s->d_hdr, sizeof(SrvEpoch)));
+    SCK(cudaMalloc(&s->d_jobs, sizeof(SrvJob) * kMaxActive));
+    SCK(cudaMalloc(&s->d_vals, kValsCap));
+    SCK(cudaMalloc(&s->d_join, sizeof(NsatJoinState)));
+    SCK(cudaMallocHost(&s->h_hdr, sizeof(SrvEpoch)));
+    SCK(cudaMallocHost(&s->h_jobs, sizeof(SrvJob) * kMaxActive));
+    SCK(cudaMallocHost(&s->h_vals, kValsCap));
+    SCK(cudaMallocHost(&s->h_join, sizeof(NsatJoinState)));
+    memset(s->h_hdr, 0, sizeof(SrvEpoch));
+    memset(s->h_jobs, 0, sizeof(SrvJob) * kMaxActive);
+    SCK(cudaEventCreate(&s->ev0));
+    SCK(cudaEventCreate(&s->ev1));
+    *out = sp.release();
+    return NSAT_OK;
+}
+
+extern "C" void nsat_server_destroy(nsat_server* s) { delete s; }
+
+extern "C" int nsat_server_submit(nsat_server* s, const nsat_job_desc* jd, uint64_t* id) {
+    if (!s || !jd || !id) return NSAT_EINVAL;
+    if (s->queue.size() >= s->opts.max_queue) return ctx_fail(s->ctx, NSAT_EBUSY, "serving queue is full");
+    if (jd->kind > 2) return NSAT_EINVAL;
+    std::unique_ptr<Job> j(new Job());
+    j->circ = circuit_from_desc(&jd->circuit);
+    for (uint32_t k = 0; k < jd->circuit.gate_num; k++)
+        if (jd->circuit.gates[3 * k] > 3) return ctx_fail(s->ctx, NSAT_EINVAL, "bad gate function");
+    std::string v = j->circ.validate();
+    if (!v.empty()) return ctx_fail(s->ctx, NSAT_EINVAL, v);
+    j->kind = jd->kind;
+    j->tag = jd->tag;
+    j->n = j->circ.n;
+    std::vector<uint32_t> which{0};
+    if (j->kind == SRV_TABLE) {
+        if (j->circ.outputs.size() != j->n + 1) return ctx_fail(s->ctx, NSAT_EINVAL, "SATOSTOP circuit needs n+1 outputs");
+        if (j->n > 28 || jd->unknowns > j->n) return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, "served SATOSTOP needs n <= 28");
+        which.clear();
+        for (uint32_t k = 0; k <= j->n; k++) which.push_back(k);
+        j->unknowns = jd->unknowns;
+        j->nb = j->n;
+        j->total_tiles = j->n > SRV_TILE_BITS ? (1ull << (j->n - SRV_TILE_BITS)) : 1;
+    } else {
+        const uint32_t d = j->n < SRV_TILE_BITS ? SRV_TILE_BITS - j->n : 0;
+        j->d = d;
+        j->nb = j->n + d;
+        if (j->nb > SRV_MAX_NB) return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, "served jobs need n <= 48");
+        j->total_tiles = 1ull << (j->nb - SRV_TILE_BITS);
+        if (j->kind == SRV_QSAT) {
+            if (!jd->quants) return NSAT_EINVAL;
+            j->quants.assign(jd->quants, jd->quants + j->n);
+            for (auto& q : j->quants) q = q ? 1 : 0;
+            const uint8_t last = j->quants[j->n - 1];
+            for (uint32_t k = 0; k < d; k++) j->quants.push_back(last ? 0 : 1);
+            uint32_t f = 0;
+            while (f < j->n && j->quants[f] == j->quants[0]) f++;
+            j->f = f;
+            j->m = j->nb - f;
+            if (j->m >= SRV_TILE_BITS)
+                j->qr.reset(new QuantReducer(std::vector<uint8_t>(j->quants.begin(), j->quants.begin() + (j->nb - SRV_TILE_BITS))));
+        }
+    }
+    std::string err;
+    if (!build_program(j->circ, which, ctx_no_optimize(s->ctx), &j->prog, &err))
+        return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, err);
+    // a job that could never be admitted is refused now rather than blocking the queue
+    auto round = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t need = round(j->prog.ins.size() * 8 + 8) + round(j->prog.outs.size() * 2 + 2) +
+                        (j->kind == SRV_TABLE ? 2 * round((size_t)8 << j->n) : 0);
+    if (need > s->arena.cap)
+        return ctx_fail(s->ctx, NSAT_ENOMEM, "job needs " + std::to_string(need) + " bytes, the server arena holds " +
+                                                 std::to_string(s->arena.cap));
+    j->slice = s->opts.first_slice_tiles;
+    j->id = s->next_id++;
+    j->res.id = j->id;
+    j->res.tag = j->tag;
+    j->res.kind = j->kind;
+    j->res.submit_ms = now_ms();
+    *id = j->id;
+    s->queue.push_back(std::move(j));
+    return NSAT_OK;
+}
+
+extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_queued) {
+    if (!s) return NSAT_EINVAL;
+    SCK(cudaSetDevice(ctx_device(s->ctx)));
+    // admission in arrival order, by device memory
+    while (!s->queue.empty() && s->active.size() < s->opts.max_active) {
+        Job* j = s->queue.front().get();
+        int a = admit(s, j);
+        if (a < 0) return a;
+        if (a > 0) break;   // does not fit yet
+        s->active.push_back(std::move(s->queue.front()));
+        s->queue.pop_front();
+    }
+    if (s->active.empty()) {
+        if (n_active) *n_active = 0;
+        if (n_queued) *n_queued = (uint32_t)s->queue.size();
+        return NSAT_OK;
+    }
+    // epoch table: slices of every active job, within the work budget
+    const uint32_t na = (uint32_t)s->active.size();
+    uint64_t budget = s->opts.epoch_budget;
+    size_t vals = 0;
+    uint32_t k = 0, slots = 32;
+    std::vector<Job*> in_epoch;
+    for (uint32_t t = 0; t < na; t++) {
+        Job* j = s->active[(s->rr + t) % na].get();
+        uint64_t want = std::min<uint64_t>(j->slice, j->total_tiles - j->cursor);
+        const uint64_t cost_per_tile = std::max<uint64_t>(1, j->prog.ins.size());
+        if (k > 0 && want * cost_per_tile > budget) want = budget / cost_per_tile;
+        if (j->kind == SRV_QSAT && j->qr) want = std::min<uint64_t>(want, kValsCap - vals);
+        if (want == 0) continue;
+        SrvJob& r = j->rec;
+        r.tile_begin = j->cursor;
+        r.tile_end = j->cursor + want;
+        r.claim = r.tile_begin;
+        r.count = 0;
+        r.min_idx = ~0ull;
+        r.any = 0;
+        r.val_off = (uint32_t)vals;
+        if (j->kind == SRV_QSAT && j->qr) vals += want;
+        budget -= std::min<uint64_t>(budget, want * cost_per_tile);
+        s->h_jobs[k++] = r;
+        slots = std::max<uint32_t>(slots, (j->prog.nslots + 31) & ~31u);
+        in_epoch.push_back(j);
+    }
+    s->rr = (s->rr + 1) % na;
+    s->h_hdr->njobs = k;
+    if (!s->graph || slots > s->graph_slots) {
+        if (int rc = capture_graph(s, std::max(slots, s->graph_slots))) return rc;
+    }
+    SCK(cudaGraphLaunch(s->graph, ctx_stream(s->ctx)));
+    SCK(cudaStreamSynchronize(ctx_stream(s->ctx)));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->device_ms += ms;
+    s->epochs++;
+    // results
+    for (uint32_t i = 0; i < k; i++) {
+        Job* j = in_epoch[i];
+        const SrvJob& r = s->h_jobs[i];
+        const uint64_t got = r.tile_end - r.tile_begin;
+        j->res.tiles += got;
+        bool finished = false;
+        if (j->kind == SRV_SAT) {
+            j->count += r.count;
+            if (r.min_idx != ~0ull) {
+                j->res.satisfiable = 1;
+                const uint64_t w = r.min_idx >> j->d;
+                j->res.witness_lo = w;
+                finished = true;
+            }
+            j->cursor = r.tile_end;
+            if (j->cursor == j->total_tiles) finished = true;
+            j->res.count = j->count >> j->d;
+        } else if (j->kind == SRV_QSAT) {
+            j->cursor = r.tile_end;
+            j->res.reversed = j->quants[0];
+            j->res.solution_bits = j->f;
+            if (!j->qr) {
+                if (r.min_idx != ~0ull) {
+                    j->res.has_solution = 1;
+                    j->res.solution = reverse_bits(r.min_idx, j->f);
+                    finished = true;
+                } else if (j->cursor == j->total_tiles) {
+                    finished = true;
+                }
+            } else {
+                for (uint64_t t = 0; t < got && !finished; t++) {
+                    j->qr->push(s->h_vals[r.val_off + t] != 0);
+                    FinalResult fr;
+                    if (j->qr->final_result(&fr)) {
+                        j->res.has_solution = fr.has_solution;
+                        j->res.solution = fr.has_solution ? fr.solution : 0;
+                        finished = true;
+                    }
+                }
+            }
+            if (finished) j->res.value = j->res.has_solution ? (j->quants[0] ? 0 : 1) : (j->quants[0] ? 1 : 0);
+        } else {
+            j->any_stop |= r.any != 0;
+            j->cursor = r.tile_end;
+            if (j->cursor == j->total_tiles) {
+                if (int rc = run_joins(s, j)) return rc;
+                finished = true;
+            }
+        }
+        j->slice = std::min<uint64_t>(j->slice * 2, s->opts.max_slice_tiles);
+        if (finished) j->finished = true;
+    }
+    // retire finished jobs
+    std::vector<std::unique_ptr<Job>> keep;
+    for (auto& jp : s->active) {
+        if (jp->finished) {
+            release(s, jp.get());
+            finish(s, jp.get());
+        } else {
+            keep.push_back(std::move(jp));
+        }
+    }
+    s->active.swap(keep);
+    if (n_active) *n_active = (uint32_t)s->active.size();
+    if (n_queued) *n_queued = (uint32_t)s->queue.size();
+    return NSAT_OK;
+}
+
+extern "C" int nsat_server_poll(nsat_server* s, nsat_job_result* out, uint32_t cap, uint32_t* n) {
+    if (!s || !n || (cap && !out)) return NSAT_EINVAL;
+    const uint32_t k = (uint32_t)std::min<size_t>(cap, s->done.size());
+    for (uint32_t i = 0; i < k; i++) out[i] = s->done[i];
+    s->done.erase(s->done.begin(), s->done.begin() + k);
+    *n = k;
+    return NSAT_OK;
+}
+
+extern "C" int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st) {
+    if (!s || !st) return NSAT_EINVAL;
+    st->epochs = s->epochs;
+    st->device_ms = s->device_ms;
+    st->active = (uint32_t)s->active.size();
+    st->queued = (uint32_t)s->queue.size();
+    st->arena_used = s->arena.used;
+    st->arena_bytes = s->arena.cap;
+    st->graph_slots = s->graph_slots;
+    st->grid = (uint32_t)s->grid;
+    return NSAT_OK;
+}

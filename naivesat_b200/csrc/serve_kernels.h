@@ -1,0 +1,12 @@
+// serve_kernels.h -- launchers of the serving engine's interpreter kernel.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "serve_common.h"
+
+extern "C" {
+int nsat_launch_serve_epoch(const SrvEpoch* hdr, SrvJob* jobs, uint32_t max_slots, uint8_t* vals, int grid,
+                            cudaStream_t stream);
+int nsat_serve_occupancy(uint32_t max_slots, int* ctas_per_sm);
+}

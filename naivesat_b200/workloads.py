@@ -10,6 +10,8 @@ Circuits are returned in the flat encoding of include/nsat.h: gates (g,3)
 Generators first build "raw" gates whose fan-ins may be negated, then fold
 those negations forward (gatesim gates have no input negation).
 """
+import math
+
 import numpy as np
 
 AND, NOR, NIMPL, XOR = 0, 1, 2, 3
@@ -94,32 +96,38 @@ class RawBuilder:
         n = self.n
         inv = [0] * (n + len(self.raw))
         gates = []
+        canon = _canonical_table()
         for k, (f, a, na, b, nb) in enumerate(self.raw):
-            ea, eb = na ^ inv[a], nb ^ inv[b]
-            tt = [_gate(f, x ^ ea, y ^ eb) for x in (0, 1) for y in (0, 1)]   # rows (x,y)
-            found = None
-            for g in (f, AND, NOR, NIMPL, XOR):
-                for swap in (0, 1):
-                    for oneg in (0, 1):
-                        ok = True
-                        for x in (0, 1):
-                            for y in (0, 1):
-                                v = _gate(g, y, x) if swap else _gate(g, x, y)
-                                if (v ^ oneg) != tt[2 * x + y]:
-                                    ok = False
-                        if ok:
-                            found = (g, swap, oneg)
-                            break
-                    if found:
-                        break
-                if found:
-                    break
-            assert found is not None
-            g, swap, oneg = found
+            g, swap, oneg = canon[(f, na ^ inv[a], nb ^ inv[b])]
             gates.append((g, b, a) if swap else (g, a, b))
             inv[n + k] = oneg
         outputs = [(w, ng ^ inv[w]) for (w, ng) in self.outs]
         return Circuit(n, gates, outputs, quants=quants, name=name)
+
+
+_CANON = None
+
+
+def _canonical_table():
+    """(func, negate i0, negate i1) -> (gatesim func, swap inputs, complement
+    output) with the same truth table over the un-negated inputs."""
+    global _CANON
+    if _CANON is None:
+        _CANON = {}
+        for f in (AND, NOR, NIMPL, XOR):
+            for ea in (0, 1):
+                for eb in (0, 1):
+                    tt = [_gate(f, x ^ ea, y ^ eb) for x in (0, 1) for y in (0, 1)]
+                    found = None
+                    for g in (f, AND, NOR, NIMPL, XOR):
+                        for swap in (0, 1):
+                            for oneg in (0, 1):
+                                if all(((_gate(g, y, x) if swap else _gate(g, x, y)) ^ oneg) == tt[2 * x + y]
+                                       for x in (0, 1) for y in (0, 1)):
+                                    found = found or (g, swap, oneg)
+                    assert found is not None
+                    _CANON[(f, ea, eb)] = found
+    return _CANON
 
 
 def random_dag_raw(rng, n, num_gates, window=64, neg_prob_quarter=True):
@@ -171,7 +179,19 @@ def last_live_gate(circ):
 def random_dag(seed, n, num_gates, window=64, output="last"):
     """Random DAG generator.  output="last": the single output is the last
     gate (config 0 as specified); output="live": the last gate that is not
-    constant on the seeded sample (used where the last gate is constant)."""
+    constant on the seeded sample (used where the last gate is constant).
+    Runs the library's generator (nsat_gen_random_dag), which is bit-identical
+    to random_dag_py below."""
+    from . import api
+    gates, outputs = api.gen_random_dag(seed, n, num_gates, window, output == "live")
+    c = Circuit(n, gates, outputs, name="dag_s%d_n%d_g%d" % (seed, n, num_gates))
+    c.out_gate = int(outputs[0][0]) - n
+    return c
+
+
+def random_dag_py(seed, n, num_gates, window=64, output="last"):
+    """Pure-Python statement of random_dag (the reference for the library's
+    generator)."""
     rng = SplitMix64(seed)
     rb = random_dag_raw(rng, n, num_gates, window)
     out = n + num_gates - 1
@@ -286,7 +306,18 @@ def _eq_chain(rb, n, pattern):
 
 
 def lfsr_stop(seed, n=24, mixer_gates=300):
-    """Config 3a: next = Fibonacci LFSR(s) XOR mixer(s), STOP = (s == P)."""
+    """Config 3a: next = Fibonacci LFSR(s) XOR mixer(s), STOP = (s == P).
+    Runs the library's generator (nsat_gen_lfsr_stop), bit-identical to
+    lfsr_stop_py below."""
+    from . import api
+    gates, outputs, pattern = api.gen_lfsr_stop(seed, n, mixer_gates)
+    c = Circuit(n, gates, outputs, name="lfsr_s%d_n%d" % (seed, n))
+    c.pattern = pattern
+    return c
+
+
+def lfsr_stop_py(seed, n=24, mixer_gates=300):
+    """Pure-Python statement of lfsr_stop."""
     rng = SplitMix64(seed)
     taps = {n - 1}
     while len(taps) < 4:
@@ -354,3 +385,41 @@ def config(name):
     if name == "c3b":
         return counter_stop(24)
     raise KeyError(name)
+
+
+def serving_requests(count, seed=2024, rate_hz=100.0, n_range=(18, 34), g_range=(100, 4000),
+                     mix=(0.7, 0.2, 0.1), stop_n_range=(12, 20)):
+    """Config 4: `count` requests with Poisson arrivals at `rate_hz`: SAT /
+    QSAT / SATOSTOP in proportions `mix`; SAT and QSAT circuits have
+    n ~ U[n_range] inputs and G ~ log-uniform[g_range] gates (the config-0
+    generator, per-request seeds, live output), QSAT quantifiers are seeded
+    random; SATOSTOP circuits are LFSR+mixer next-state circuits with
+    n ~ U[stop_n_range] state bits and the top n/2 bits unknown."""
+    rng = SplitMix64(seed)
+    reqs = []
+    t = 0.0
+    for i in range(count):
+        # exponential inter-arrival time from a uniform in (0, 1]
+        u = (rng.next() >> 11) / float(1 << 53)
+        t += -math.log(1.0 - u) / rate_hz if u < 1.0 else 0.0
+        r = (rng.next() >> 11) / float(1 << 53)
+        kind = "sat" if r < mix[0] else "qsat" if r < mix[0] + mix[1] else "stop"
+        rseed = rng.next() & 0xFFFFFFFF
+        if kind == "stop":
+            n = stop_n_range[0] + rng.below(stop_n_range[1] - stop_n_range[0] + 1)
+            g = int(math.exp(math.log(50) + (rng.next() >> 11) / float(1 << 53) * (math.log(1000) - math.log(50))))
+            c = lfsr_stop(rseed, n, max(g, n + 1))
+            reqs.append({"arrival_s": t, "kind": "stop", "circ": c, "quants": None, "unknowns": n // 2,
+                         "seed": rseed})
+            continue
+        n = n_range[0] + rng.below(n_range[1] - n_range[0] + 1)
+        lg = math.log(g_range[0]) + (rng.next() >> 11) / float(1 << 53) * (math.log(g_range[1]) - math.log(g_range[0]))
+        g = int(math.exp(lg))
+        c = random_dag(rseed, n, g, output="live")
+        quants = None
+        if kind == "qsat":
+            qr = SplitMix64(rseed ^ 0xA5A5)
+            quants = "".join("A" if qr.below(2) else "E" for _ in range(n))
+            c.quants = quants
+        reqs.append({"arrival_s": t, "kind": kind, "circ": c, "quants": quants, "unknowns": 0, "seed": rseed})
+    return reqs

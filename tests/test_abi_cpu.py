@@ -102,3 +102,18 @@ def test_lut_mapping_saves_ops():
     c = W.config("c1")
     fused = api.jit_check(c, "sat")
     assert fused["lop3_ops"] < 0.8 * fused["live_gates"], fused
+
+
+@pytest.mark.parametrize("seed,n,g,out", [(0, 24, 500, "last"), (1, 36, 3000, "live"), (3, 30, 1500, "live"),
+                                          (77, 18, 100, "last"), (123456789, 34, 4000, "live")])
+def test_library_generator_matches_python(seed, n, g, out):
+    a = W.random_dag(seed, n, g, output=out)
+    b = W.random_dag_py(seed, n, g, output=out)
+    assert (a.gates == b.gates).all() and (a.outputs == b.outputs).all()
+
+
+@pytest.mark.parametrize("seed,n,g", [(4, 24, 300), (4, 32, 300), (99, 15, 120)])
+def test_library_lfsr_generator_matches_python(seed, n, g):
+    a = W.lfsr_stop(seed, n, g)
+    b = W.lfsr_stop_py(seed, n, g)
+    assert (a.gates == b.gates).all() and (a.outputs == b.outputs).all() and a.pattern == b.pattern

@@ -1,0 +1,95 @@
+"""Batched serving (nsat_server_*): every job's answer in a mixed batch
+equals the oracle's and equals the same job served alone."""
+import pytest
+
+from naivesat_b200 import api
+from naivesat_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def small_mix(count, seed):
+    return W.serving_requests(count, seed=seed, rate_hz=1e9, n_range=(12, 22), g_range=(40, 600),
+                              stop_n_range=(8, 14))
+
+
+def expected(req):
+    c = req["circ"]
+    oc = O.Circuit(c.n, c.gates, c.outputs)
+    if req["kind"] == "sat":
+        cnt, low = O.sat_range(oc)
+        return {"satisfiable": low is not None, "witness": low}
+    if req["kind"] == "qsat":
+        r = O.qsat(oc, req["quants"], mode=1)
+        return {"reversed": r["reversed"], "solution_bits": r["solution_bits"], "solution": r["solution"]}
+    r = O.stop_solve(c.n, req["unknowns"], O.stop_table(oc), mode=1)
+    if r is None:
+        return {"found": False}
+    return {"found": True, "start": r["start"], "end": r["end"], "steps": r["steps"]}
+
+
+def project(res, exp):
+    return {k: res[k] for k in exp}
+
+
+def submit_all(srv, reqs):
+    ids = {}
+    for i, r in enumerate(reqs):
+        ids[srv.submit(r["kind"], r["circ"], quants=r["quants"], unknowns=r["unknowns"], tag=i)] = i
+    return ids
+
+
+def test_mixed_batch_matches_oracle_and_alone(ctx):
+    reqs = small_mix(48, 11)
+    srv = api.Server(ctx)
+    submit_all(srv, reqs)
+    res = {r["tag"]: r for r in srv.run_all()}
+    assert len(res) == len(reqs)
+    for i, r in enumerate(reqs):
+        exp = expected(r)
+        assert project(res[i], exp) == exp, (i, r["kind"], res[i], exp)
+    # the same jobs, each alone
+    for i in range(0, len(reqs), 3):
+        alone = api.Server(ctx)
+        alone.submit(reqs[i]["kind"], reqs[i]["circ"], quants=reqs[i]["quants"], unknowns=reqs[i]["unknowns"])
+        got = alone.run_all()[0]
+        exp = expected(reqs[i])
+        assert project(got, exp) == project(res[i], exp)
+        alone.close()
+
+
+def test_large_jobs_match_one_shot_solvers(ctx):
+    """n = 26..30 jobs against the compiled one-shot solvers (the oracle would
+    be slow here); slices span many epochs."""
+    reqs = W.serving_requests(6, seed=5, rate_hz=1e9, n_range=(26, 30), g_range=(200, 1200), mix=(0.5, 0.5, 0.0))
+    srv = api.Server(ctx)
+    submit_all(srv, reqs)
+    res = {r["tag"]: r for r in srv.run_all()}
+    for i, r in enumerate(reqs):
+        h = ctx.circuit(r["circ"])
+        if r["kind"] == "sat":
+            one = h.sat(find_all=False)
+            assert (res[i]["satisfiable"], res[i]["witness"]) == (one["satisfiable"], one["witness"])
+        else:
+            one = h.qsat(r["quants"])
+            assert (res[i]["reversed"], res[i]["solution_bits"], res[i]["solution"]) == \
+                (one["reversed"], one["solution_bits"], one["solution"])
+
+
+def test_admission_by_memory_and_queue_limit(ctx):
+    reqs = [r for r in small_mix(40, 23) if r["kind"] == "stop"][:4]
+    assert reqs
+    # room for about one table at a time: the rest wait in the queue
+    srv = api.Server(ctx, arena_bytes=2 * 8 * (1 << 14) + 65536, max_queue=3)
+    submitted = 0
+    with pytest.raises(api.NsatError, match="EBUSY"):
+        for r in reqs + reqs:
+            srv.submit(r["kind"], r["circ"], unknowns=r["unknowns"], tag=submitted)
+            submitted += 1
+    assert submitted == 3
+    res = srv.run_all()
+    assert len(res) == 3
+    for r in res:
+        exp = expected(reqs[r["tag"] % len(reqs)])
+        assert project(r, exp) == exp
