@@ -240,7 +240,11 @@ typedef struct {
     const uint8_t* quants;      /* QSAT: one per input, 1 = All */
     nsat_circuit_desc circuit;
     uint64_t tag;               /* returned with the result */
+    uint32_t flags;             /* NSAT_JOB_FIND_ALL: a SAT job counts every solution */
+    uint32_t reserved;
 } nsat_job_desc;
+
+#define NSAT_JOB_FIND_ALL 1u
 
 typedef struct {
     uint64_t id, tag;
@@ -277,6 +281,15 @@ int nsat_server_step(nsat_server* s, uint32_t* active, uint32_t* queued);
 /* Moves up to `cap` finished results to `out`. */
 int nsat_server_poll(nsat_server* s, nsat_job_result* out, uint32_t cap, uint32_t* n);
 int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st);
+
+/* Host-only check of the interpreter program a job of `kind` would get:
+ * builds it, runs it on the host with the kernel's group semantics (a
+ * group's operands are read before any of its results is written) for two
+ * passes of 64 seeded random assignments, and compares every requested
+ * output with direct evaluation of the circuit.  Reports the program's
+ * slots, LUTs and padding NOPs.  NSAT_EINVAL on a mismatch.  Needs no GPU. */
+int nsat_server_program_check(const nsat_circuit_desc* circuit, uint32_t kind, uint64_t seed,
+                              uint32_t* slots, uint32_t* luts, uint32_t* nops);
 
 /* ---- seeded benchmark circuits ------------------------------------------- */
 /* Random DAG of the benchmark configurations: `gates` two-input gates, types

@@ -6,6 +6,7 @@ the calls raise.
 """
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -84,7 +85,8 @@ class ServerOpts(C.Structure):
 
 class JobDesc(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("unknowns", C.c_uint32), ("quants", U8P),
-                ("circuit", CircuitDesc), ("tag", C.c_uint64)]
+                ("circuit", CircuitDesc), ("tag", C.c_uint64), ("flags", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class JobResult(C.Structure):
@@ -111,7 +113,7 @@ EXPORTS = [
     "nsat_table_bytes", "nsat_stop_solve", "nsat_probe_lop3_peak", "nsat_jit_check",
     "nsat_qsat_solve_noalloc", "nsat_server_create", "nsat_server_destroy", "nsat_server_submit",
     "nsat_server_step", "nsat_server_poll", "nsat_server_stats", "nsat_gen_random_dag",
-    "nsat_gen_lfsr_stop",
+    "nsat_gen_lfsr_stop", "nsat_server_program_check",
 ]
 
 _lib = None
@@ -165,6 +167,8 @@ def lib():
         L.nsat_server_step.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.nsat_server_poll.argtypes = [C.c_void_p, C.POINTER(JobResult), C.c_uint32, C.POINTER(C.c_uint32)]
         L.nsat_server_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.nsat_server_program_check.argtypes = [C.POINTER(CircuitDesc), C.c_uint32, C.c_uint64, U32P, U32P,
+                                                U32P]
         L.nsat_gen_random_dag.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, U32P,
                                           C.c_uint32, U32P, C.c_uint32, U32P, U32P]
         L.nsat_gen_lfsr_stop.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, U32P, C.c_uint32, U32P,
@@ -208,6 +212,8 @@ class Context:
         if rc != NSAT_OK:
             raise NsatError("nsat_create(%d): %s" % (device, L.nsat_strerror(rc).decode()))
         self.h = h
+        # objects whose C handles refer to this context; closed before it
+        self._children = weakref.WeakSet()
 
     def _check(self, rc, what):
         if rc != NSAT_OK:
@@ -216,6 +222,8 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
+            for child in list(self._children):
+                child.close()
             lib().nsat_destroy(self.h)
             self.h = None
 
@@ -326,6 +334,7 @@ class Server:
         ctx._check(lib().nsat_server_create(ctx.h, C.byref(o), C.byref(h)), "server_create")
         self.h = h
         self._buf = (JobResult * 256)()
+        ctx._children.add(self)
 
     def close(self):
         if getattr(self, "h", None):
@@ -335,12 +344,15 @@ class Server:
     def __del__(self):
         self.close()
 
-    def submit(self, kind, circ, quants=None, unknowns=0, tag=0):
+    def submit(self, kind, circ, quants=None, unknowns=0, tag=0, find_all=False):
         """kind: 'sat' | 'qsat' | 'stop'.  Returns the job id (raises NsatError
-        with EBUSY when the queue is full)."""
+        with EBUSY when the queue is full).  find_all: a SAT job enumerates
+        every assignment and reports the exact count (otherwise it ends at
+        the lowest witness and the count covers the tiles evaluated)."""
         d = desc_of(circ.n, circ.gates, circ.outputs)
         q = _quants_array(quants, circ.n) if quants is not None else None
-        jd = JobDesc(KINDS[kind], unknowns, q.ctypes.data_as(U8P) if q is not None else None, d, tag)
+        jd = JobDesc(KINDS[kind], unknowns, q.ctypes.data_as(U8P) if q is not None else None, d, tag,
+                     1 if find_all else 0, 0)
         jid = C.c_uint64()
         self.ctx._check(lib().nsat_server_submit(self.h, C.byref(jd), C.byref(jid)), "server_submit")
         return jid.value
@@ -397,11 +409,15 @@ class Table:
         self.ctx._check(lib().nsat_stop_table_build(self.ctx.h, circ.h, C.byref(o), C.byref(h)),
                         "stop_table_build")
         self.h = h
+        self.ctx._children.add(self)
 
-    def __del__(self):
+    def close(self):
         if getattr(self, "h", None):
             lib().nsat_table_free(self.h)
             self.h = None
+
+    def __del__(self):
+        self.close()
 
     def read(self, first=0, count=None):
         if count is None:
@@ -463,6 +479,18 @@ def format_circuit(n, gates, outputs, quants=None):
 
 
 KIND = {"sat": 0, "qsat": 1, "table": 2}
+
+
+def server_program_check(circ, kind="sat", seed=1):
+    """Host-only check of a job's interpreter program (include/nsat.h
+    nsat_server_program_check); returns (slots, luts, nops), raises on a
+    mismatch."""
+    d = desc_of(circ.n, circ.gates, circ.outputs)
+    sl, lu, no = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    rc = lib().nsat_server_program_check(C.byref(d), KINDS[kind], seed, C.byref(sl), C.byref(lu), C.byref(no))
+    if rc != 0:
+        raise NsatError("server_program_check: %s" % lib().nsat_strerror(rc).decode(), rc)
+    return sl.value, lu.value, no.value
 
 
 def jit_check(circ, kind="sat", quants=None, block_threads=0, no_optimize=False):

@@ -15,11 +15,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -82,44 +84,114 @@ struct Arena {
     }
 };
 
-// LUT cover of the requested outputs, slot-allocated: inputs keep slots
-// 0..n-1 for the whole tile, gate values reuse slots after their last use.
+// LUT cover of the requested outputs as an interpreter program:
+// - scheduled into groups of SRV_GROUP instructions none of which reads
+//   another's result (the kernel loads a whole group's operands before it
+//   stores any result): each group takes the lowest-numbered ready LUTs, so
+//   the original topological order, and with it the live set, is kept; a NOP
+//   on a scratch slot fills a group that finds too few ready LUTs;
+// - slot-allocated by liveness over the groups.  Inputs start in slots
+//   0..n-1 (the kernel rewrites them every pass), and every slot, an input's
+//   included, is reused after the group that reads it last.
 struct Program {
-    std::vector<uint64_t> ins;
+    std::vector<SrvIns> ins;
     std::vector<uint16_t> outs;
     uint32_t nslots = 0;
+    uint32_t luts = 0;
+    uint32_t nops = 0;
 };
 
 bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool raw, Program* p, std::string* err) {
     LutNet net = map_luts(c, which, raw);
     const uint32_t W = c.wires();
+    const size_t L = net.luts.size();
+    std::vector<int32_t> lut_of(W, -1);
+    for (size_t k = 0; k < L; k++) lut_of[net.luts[k].wire] = (int32_t)k;
+    auto distinct_in = [&](const Lut& X, int i) {
+        for (int j = 0; j < i; j++)
+            if (X.in[j] == X.in[i]) return false;
+        return true;
+    };
+    std::vector<std::vector<uint32_t>> users(L);
+    std::vector<uint32_t> pending(L, 0);
+    for (size_t k = 0; k < L; k++) {
+        const Lut& X = net.luts[k];
+        for (int i = 0; i < 3; i++) {
+            const int32_t q = lut_of[X.in[i]];
+            if (q >= 0 && distinct_in(X, i)) { users[q].push_back((uint32_t)k); pending[k]++; }
+        }
+    }
+    // groups of LUT indices (-1: NOP)
+    std::set<uint32_t> ready;
+    for (size_t k = 0; k < L; k++) if (!pending[k]) ready.insert((uint32_t)k);
+    std::vector<std::array<int64_t, SRV_GROUP>> groups;
+    size_t done = 0;
+    while (done < L) {
+        std::array<int64_t, SRV_GROUP> grp;
+        grp.fill(-1);
+        int used = 0;
+        while (used < SRV_GROUP && !ready.empty()) {
+            grp[used++] = *ready.begin();
+            ready.erase(ready.begin());
+        }
+        for (int k = 0; k < used; k++) {
+            for (uint32_t u : users[grp[k]]) if (--pending[u] == 0) ready.insert(u);
+        }
+        p->nops += SRV_GROUP - used;
+        done += used;
+        groups.push_back(grp);
+    }
+    // slot allocation over the groups
     std::vector<int64_t> last(W, -1);
-    for (size_t k = 0; k < net.luts.size(); k++)
-        for (int i = 0; i < 3; i++) last[net.luts[k].in[i]] = (int64_t)k;
+    for (size_t g = 0; g < groups.size(); g++)
+        for (int64_t q : groups[g])
+            if (q >= 0) for (int i = 0; i < 3; i++) last[net.luts[q].in[i]] = (int64_t)g;
     for (const Output& o : net.outs) last[o.wire] = INT64_MAX;
     std::vector<int32_t> slot(W, -1);
     for (uint32_t i = 0; i < c.n; i++) slot[i] = (int32_t)i;
     uint32_t next = c.n;
     std::vector<uint32_t> freel;
+    for (uint32_t i = c.n; i-- > 0;) if (last[i] < 0) freel.push_back(i);   // unread inputs
+    const uint32_t scratch = next++;       // NOP operands and target
     p->ins.clear();
-    for (size_t k = 0; k < net.luts.size(); k++) {
-        const Lut& L = net.luts[k];
-        uint32_t d;
-        if (!freel.empty()) { d = freel.back(); freel.pop_back(); }
-        else d = next++;
-        slot[L.wire] = (int32_t)d;
-        p->ins.push_back((uint64_t)slot[L.in[0]] | ((uint64_t)slot[L.in[1]] << 12) | ((uint64_t)slot[L.in[2]] << 24) |
-                         ((uint64_t)d << 36) | ((uint64_t)L.tt << 48));
-        // free gate slots whose last use is this LUT (after the write: no aliasing)
-        for (int i = 0; i < 3; i++) {
-            const uint32_t w = L.in[i];
-            if (w >= c.n && last[w] == (int64_t)k) {
-                bool dup = false;
-                for (int j = 0; j < i; j++) dup |= (L.in[j] == w);
-                if (!dup) freel.push_back((uint32_t)slot[w]);
+    p->ins.reserve(groups.size() * SRV_GROUP);
+    for (size_t g = 0; g < groups.size(); g++) {
+        // operands read for the last time in this group free their slots first
+        for (int64_t q : groups[g]) {
+            if (q < 0) continue;
+            const Lut& X = net.luts[q];
+            for (int i = 0; i < 3; i++) {
+                const uint32_t w = X.in[i];
+                if (last[w] == (int64_t)g) {
+                    freel.push_back((uint32_t)slot[w]);
+                    last[w] = -2;   // freed once, however many readers this group has
+                }
             }
         }
+        for (int64_t q : groups[g]) {
+            uint32_t a = scratch, b = scratch, cc = scratch, d = scratch, tt = 0;
+            if (q >= 0) {
+                const Lut& X = net.luts[q];
+                if (!freel.empty()) { d = freel.back(); freel.pop_back(); }
+                else d = next++;
+                slot[X.wire] = (int32_t)d;
+                a = (uint32_t)slot[X.in[0]];
+                b = (uint32_t)slot[X.in[1]];
+                cc = (uint32_t)slot[X.in[2]];
+                tt = X.tt;
+            }
+            SrvIns r;
+            r.ab = a | b << 16;
+            r.cd = cc | d << 16;
+            r.tlo = r.thi = 0;
+            for (int k = 0; k < 4; k++) {
+                r.tlo |= ((tt >> k) & 1u) << (8 * k + 7);
+                r.thi |= ((tt >> (k + 4)) & 1u) << (8 * k + 7);
+            }
+            p->ins.push_back(r);
+        }
     }
+    p->luts = (uint32_t)L;
     p->nslots = next;
     if (next > SRV_MAX_SLOTS) {
         *err = "circuit needs " + std::to_string(next) + " slots, the interpreter holds " +
@@ -145,6 +217,7 @@ struct Job {
     SrvJob rec{};
     size_t prog_off = 0, outs_off = 0, table_off = 0, table2_off = 0, reserve = 0;
     bool any_stop = false;
+    bool find_all = false;
     bool finished = false;
     uint64_t count = 0;
     nsat_job_result res{};
@@ -215,9 +288,7 @@ int capture_graph(nsat_server* s, uint32_t slots) {
     SCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(s->d_hdr, s->h_hdr, sizeof(SrvEpoch), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(s->d_jobs, s->h_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyHostToDevice, st);
-    cudaEventRecord(s->ev0, st);
     int rc = nsat_launch_serve_epoch(s->d_hdr, s->d_jobs, slots, s->d_vals, s->grid, st);
-    cudaEventRecord(s->ev1, st);
     cudaMemcpyAsync(s->h_jobs, s->d_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(s->h_vals, s->d_vals, kValsCap, cudaMemcpyDeviceToHost, st);
     cudaError_t ce = cudaStreamEndCapture(st, &g);
@@ -238,30 +309,34 @@ void finish(nsat_server* s, Job* j) {
     s->done.push_back(j->res);
 }
 
+size_t prog_bytes(const Job* j) { return j->prog.ins.size() * sizeof(SrvIns) + sizeof(SrvIns); }
+size_t outs_bytes(const Job* j) { return j->prog.outs.size() * 2 + 2; }
+size_t table_bytes(const Job* j) { return j->kind == SRV_TABLE ? ((size_t)8 << j->n) : 0; }
+
 int admit(nsat_server* s, Job* j) {
-    const size_t pbytes = j->prog.ins.size() * 8 + 8, obytes = j->prog.outs.size() * 2 + 2;
-    size_t tbytes = j->kind == SRV_TABLE ? ((size_t)8 << j->n) : 0;
-    if (!s->arena.alloc(pbytes, &j->prog_off)) return 1;
-    if (!s->arena.alloc(obytes, &j->outs_off)) { s->arena.release(j->prog_off, pbytes); return 1; }
-    if (tbytes) {
-        if (!s->arena.alloc(tbytes, &j->table_off)) {
-            s->arena.release(j->prog_off, pbytes); s->arena.release(j->outs_off, obytes); return 1;
-        }
-        if (!s->arena.alloc(tbytes, &j->table2_off)) {
-            s->arena.release(j->prog_off, pbytes); s->arena.release(j->outs_off, obytes);
-            s->arena.release(j->table_off, tbytes); return 1;
+    const size_t pbytes = prog_bytes(j), obytes = outs_bytes(j), tbytes = table_bytes(j);
+    size_t offs[4] = {0, 0, 0, 0};
+    const size_t sizes[4] = {pbytes, obytes, tbytes, tbytes};
+    const int parts = tbytes ? 4 : 2;
+    for (int i = 0; i < parts; i++) {
+        if (!s->arena.alloc(sizes[i], &offs[i])) {
+            for (int k = 0; k < i; k++) s->arena.release(offs[k], sizes[k]);
+            return 1;
         }
     }
+    j->prog_off = offs[0]; j->outs_off = offs[1];
+    j->table_off = offs[2]; j->table2_off = offs[3];
     j->reserve = pbytes + obytes + 2 * tbytes;
     cudaStream_t st = ctx_stream(s->ctx);
-    SCK(cudaMemcpyAsync(s->arena.base + j->prog_off, j->prog.ins.data(), j->prog.ins.size() * 8, cudaMemcpyHostToDevice, st));
+    SCK(cudaMemcpyAsync(s->arena.base + j->prog_off, j->prog.ins.data(), j->prog.ins.size() * sizeof(SrvIns),
+                        cudaMemcpyHostToDevice, st));
     SCK(cudaMemcpyAsync(s->arena.base + j->outs_off, j->prog.outs.data(), j->prog.outs.size() * 2, cudaMemcpyHostToDevice, st));
     SrvJob& r = j->rec;
     memset(&r, 0, sizeof(r));
-    r.prog = (const srv_u64*)(s->arena.base + j->prog_off);
+    r.prog = (const SrvIns*)(s->arena.base + j->prog_off);
     r.outs = (const uint16_t*)(s->arena.base + j->outs_off);
     r.table = tbytes ? (srv_u64*)(s->arena.base + j->table_off) : nullptr;
-    r.ninstr = (uint32_t)j->prog.ins.size();
+    r.ngroups = (uint32_t)(j->prog.ins.size() / SRV_GROUP);
     r.nslots = j->prog.nslots;
     r.kind = j->kind;
     r.nb = j->nb;
@@ -289,13 +364,11 @@ int admit(nsat_server* s, Job* j) {
 }
 
 void release(nsat_server* s, Job* j) {
-    const size_t pbytes = j->prog.ins.size() * 8 + 8, obytes = j->prog.outs.size() * 2 + 2;
-    s->arena.release(j->prog_off, pbytes);
-    s->arena.release(j->outs_off, obytes);
+    s->arena.release(j->prog_off, prog_bytes(j));
+    s->arena.release(j->outs_off, outs_bytes(j));
     if (j->kind == SRV_TABLE) {
-        const size_t tbytes = (size_t)8 << j->n;
-        s->arena.release(j->table_off, tbytes);
-        s->arena.release(j->table2_off, tbytes);
+        s->arena.release(j->table_off, table_bytes(j));
+        s->arena.release(j->table2_off, table_bytes(j));
     }
 }
 
@@ -381,6 +454,7 @@ extern "C" int nsat_server_submit(nsat_server* s, const nsat_job_desc* jd, uint6
     if (!v.empty()) return ctx_fail(s->ctx, NSAT_EINVAL, v);
     j->kind = jd->kind;
     j->tag = jd->tag;
+    j->find_all = (jd->flags & NSAT_JOB_FIND_ALL) != 0;
     j->n = j->circ.n;
     std::vector<uint32_t> which{0};
     if (j->kind == SRV_TABLE) {
@@ -416,8 +490,8 @@ extern "C" int nsat_server_submit(nsat_server* s, const nsat_job_desc* jd, uint6
         return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, err);
     // a job that could never be admitted is refused now rather than blocking the queue
     auto round = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t need = round(j->prog.ins.size() * 8 + 8) + round(j->prog.outs.size() * 2 + 2) +
-                        (j->kind == SRV_TABLE ? 2 * round((size_t)8 << j->n) : 0);
+    const size_t need = round(prog_bytes(j.get())) + round(outs_bytes(j.get())) +
+                        2 * round(table_bytes(j.get()));
     if (need > s->arena.cap)
         return ctx_fail(s->ctx, NSAT_ENOMEM, "job needs " + std::to_string(need) + " bytes, the server arena holds " +
                                                  std::to_string(s->arena.cap));
@@ -453,7 +527,7 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
     const uint32_t na = (uint32_t)s->active.size();
     uint64_t budget = s->opts.epoch_budget;
     size_t vals = 0;
-    uint32_t k = 0, slots = 32;
+    uint32_t k = 0, slots = 16;
     std::vector<Job*> in_epoch;
     for (uint32_t t = 0; t < na; t++) {
         Job* j = s->active[(s->rr + t) % na].get();
@@ -473,7 +547,7 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
         if (j->kind == SRV_QSAT && j->qr) vals += want;
         budget -= std::min<uint64_t>(budget, want * cost_per_tile);
         s->h_jobs[k++] = r;
-        slots = std::max<uint32_t>(slots, (j->prog.nslots + 31) & ~31u);
+        slots = std::max<uint32_t>(slots, (j->prog.nslots + 15) & ~15u);
         in_epoch.push_back(j);
     }
     s->rr = (s->rr + 1) % na;
@@ -481,10 +555,13 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
     if (!s->graph || slots > s->graph_slots) {
         if (int rc = capture_graph(s, std::max(slots, s->graph_slots))) return rc;
     }
+    // epoch time: events around the graph replay (table copies included)
+    SCK(cudaEventRecord(s->ev0, ctx_stream(s->ctx)));
     SCK(cudaGraphLaunch(s->graph, ctx_stream(s->ctx)));
+    SCK(cudaEventRecord(s->ev1, ctx_stream(s->ctx)));
     SCK(cudaStreamSynchronize(ctx_stream(s->ctx)));
     float ms = 0;
-    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    SCK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     s->device_ms += ms;
     s->epochs++;
     // results
@@ -496,11 +573,11 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
         bool finished = false;
         if (j->kind == SRV_SAT) {
             j->count += r.count;
-            if (r.min_idx != ~0ull) {
+            if (r.min_idx != ~0ull && !j->res.satisfiable) {
+                // the first slice with a solution holds the lowest one
                 j->res.satisfiable = 1;
-                const uint64_t w = r.min_idx >> j->d;
-                j->res.witness_lo = w;
-                finished = true;
+                j->res.witness_lo = r.min_idx >> j->d;
+                if (!j->find_all) finished = true;
             }
             j->cursor = r.tile_end;
             if (j->cursor == j->total_tiles) finished = true;
@@ -575,5 +652,64 @@ extern "C" int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st) {
     st->arena_bytes = s->arena.cap;
     st->graph_slots = s->graph_slots;
     st->grid = (uint32_t)s->grid;
+    return NSAT_OK;
+}
+
+extern "C" int nsat_server_program_check(const nsat_circuit_desc* cd, uint32_t kind, uint64_t seed, uint32_t* slots,
+                                         uint32_t* luts, uint32_t* nops) {
+    if (!cd || kind > 2) return NSAT_EINVAL;
+    Circuit c = circuit_from_desc(cd);
+    if (!c.validate().empty()) return NSAT_EINVAL;
+    std::vector<uint32_t> which;
+    if (kind == SRV_TABLE) for (uint32_t k = 0; k < c.outputs.size(); k++) which.push_back(k);
+    else which.push_back(0);
+    Program p;
+    std::string err;
+    if (!build_program(c, which, false, &p, &err)) return NSAT_EUNSUPPORTED;
+    if (slots) *slots = p.nslots;
+    if (luts) *luts = p.luts;
+    if (nops) *nops = p.nops;
+    uint64_t st = seed;
+    auto rnd = [&st]() {
+        st += 0x9E3779B97F4A7C15ull;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    // slot values persist across passes, as in the kernel's shared memory
+    std::vector<uint64_t> sv(p.nslots, 0);
+    for (auto& v : sv) v = rnd();
+    for (int pass = 0; pass < 2; pass++) {
+        std::vector<uint64_t> wv(c.wires(), 0);
+        for (uint32_t i = 0; i < c.n; i++) sv[i] = wv[i] = rnd();
+        for (size_t k = 0; k < c.gates.size(); k++) {
+            const Gate& g = c.gates[k];
+            const uint64_t a = wv[g.i0], b = wv[g.i1];
+            wv[c.n + k] = g.func == AND ? (a & b) : g.func == NOR ? ~(a | b) : g.func == NIMPL ? (a & ~b) : (a ^ b);
+        }
+        for (size_t g0 = 0; g0 < p.ins.size(); g0 += SRV_GROUP) {
+            uint64_t d[SRV_GROUP];
+            for (int k = 0; k < SRV_GROUP; k++) {
+                const SrvIns& r = p.ins[g0 + k];
+                const uint64_t a = sv[r.ab & 0xffff], b = sv[r.ab >> 16], cc = sv[r.cd & 0xffff];
+                uint64_t y = 0;
+                for (int t = 0; t < 8; t++) {
+                    const uint64_t sel = ((t & 4) ? a : ~a) & ((t & 2) ? b : ~b) & ((t & 1) ? cc : ~cc);
+                    const uint32_t word = t < 4 ? r.tlo : r.thi;
+                    y |= sel & (((word >> (8 * (t & 3) + 7)) & 1) ? ~0ull : 0ull);
+                }
+                d[k] = y;
+            }
+            for (int k = 0; k < SRV_GROUP; k++) sv[p.ins[g0 + k].cd >> 16] = d[k];
+        }
+        for (size_t j = 0; j < which.size(); j++) {
+            const Output& o = c.outputs[which[j]];
+            const uint16_t os = p.outs[j];
+            const uint64_t got = sv[os & 0x7fff] ^ ((os & 0x8000) ? ~0ull : 0ull);
+            const uint64_t exp = wv[o.wire] ^ (o.neg ? ~0ull : 0ull);
+            if (got != exp) return NSAT_EINVAL;
+        }
+    }
     return NSAT_OK;
 }

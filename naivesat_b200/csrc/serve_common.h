@@ -2,17 +2,36 @@
 // bytecode interpreter kernel (serve_kernels.cu).
 #pragma once
 #include <stdint.h>
+#include <vector_types.h>
 
-// One instruction of a circuit program: a 3-input LUT over slots
-//   slot[d] = lut(slot[a], slot[b], slot[c]) with truth table tt
-// (bit (x<<2 | y<<1 | z) of tt is the value for a=x, b=y, c=z).
-// Packed as a | b<<12 | c<<24 | d<<36 | tt<<48.
-#define SRV_SLOT_BITS 12
-#define SRV_MAX_SLOTS 256          // shared-memory slots per lane the interpreter supports
-#define SRV_TILE_BITS 15           // assignments per warp tile (32 iterations x 1024)
+// Geometry of the interpreter: each lane evaluates SRV_WORDS 32-bit words
+// per program pass (SRV_WORDS * 1024 assignments per warp), and a tile of
+// 2^SRV_TILE_BITS assignments takes 32 / SRV_WORDS passes.  A slot of a warp
+// is SRV_SLOT_BYTES of shared memory laid out [lane][word].
+#ifndef SRV_WORDS
+#define SRV_WORDS 4
+#endif
+#ifndef SRV_GROUP
+#define SRV_GROUP 4               // instructions issued together (mutually independent)
+#endif
+#define SRV_LOG_WORDS (SRV_WORDS == 4 ? 2 : 1)
+#define SRV_SLOT_BYTES (32 * SRV_WORDS * 4)
+#define SRV_MAX_SLOTS 384          // slots per warp (384 x 512 B = 192 KB of shared memory)
+#define SRV_TILE_BITS 15           // assignments per warp tile
 #define SRV_MAX_NB 48              // enumeration bits a serving job may have
 
-#define SRV_WARPS_PER_CTA 4
+// One instruction: slot[d] = LUT(slot[a], slot[b], slot[c]), 16 bytes:
+//   ab = a | b << 16, cd = c | d << 16   (slot indices)
+//   tlo, thi: the truth table tt (bit x<<2 | y<<1 | z is the value for
+//   a=x, b=y, c=z) spread so that bit k of tt is the sign bit of byte k of
+//   the 8-byte pair {thi, tlo}; the kernel expands mask k (all ones or all
+//   zeros) with one byte permute that replicates that sign bit.
+// Programs are sequences of groups of SRV_GROUP instructions none of which
+// reads another's result.
+struct SrvIns {
+    uint32_t ab, cd, tlo, thi;
+};
+static_assert(sizeof(SrvIns) == 16, "SrvIns layout");
 
 enum { SRV_SAT = 0, SRV_QSAT = 1, SRV_TABLE = 2 };
 
@@ -28,10 +47,11 @@ typedef unsigned long long srv_u64;   // the device atomics' 64-bit type
 
 struct SrvJob {
     // static
-    const srv_u64* prog;        // instructions
+    const SrvIns* prog;          // ngroups * SRV_GROUP instructions
+    const void* unused0;
     const uint16_t* outs;        // output slots (bit 15 = negated), nout of them
     srv_u64* table;             // TABLE: 2^np u64 entries (next|STOP<<n | 1<<32)
-    uint32_t ninstr;
+    uint32_t ngroups;
     uint32_t nslots;
     uint32_t kind;               // SRV_SAT / SRV_QSAT / SRV_TABLE
     uint32_t nb;                 // enumeration bits (padding included)
@@ -52,7 +72,7 @@ struct SrvJob {
     srv_u64 min_idx;            // SAT: lowest witness; QSAT (m < tile bits): lowest decisive unit
     uint32_t any;                // TABLE: some state has STOP
     uint32_t pad1;
-    srv_u64 reserved[11];
+    srv_u64 reserved[10];
 };
 
 static_assert(sizeof(SrvJob) == 256, "SrvJob layout");

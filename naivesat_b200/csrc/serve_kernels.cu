@@ -4,11 +4,21 @@
 // Per-request NVRTC compilation costs 0.1-1.5 s per circuit, far more than
 // the device work of most serving requests, so serving does not specialise
 // kernels: every job is a program of 3-input LUT instructions over "slots"
-// (the LUT cover of its circuit, slot-allocated by liveness).  Each warp
-// evaluates 32 words (1024 assignments) per iteration and 32 iterations per
-// tile (2^15 assignments); slot values live in shared memory laid out
-// [slot][lane] (conflict-free), each instruction is applied with a runtime
-// truth table through a 7-LOP3 mux tree over warp-uniform masks.
+// (the LUT cover of its circuit, scheduled into groups of independent
+// instructions and slot-allocated by liveness).  A CTA is one warp; each lane
+// evaluates SRV_WORDS words per program pass, and slot values live in the
+// warp's shared memory laid out [slot][lane][word] (128-bit accesses,
+// conflict-free).  A LUT with a run-time truth table is a 7-lop3 mux tree
+// over the eight truth-table masks of the instruction record.
+//
+// Cost per instruction and warp: 3 x 128-bit shared loads, one 128-bit
+// shared store, one uniform 128-bit load of the 16-byte record, 8 byte
+// permutes that expand the truth table into masks, and 7 * SRV_WORDS lop3.
+// The L1 data pipe moves 512 bytes per 128-bit warp access, so the record is
+// kept at 16 bytes (a record of eight mask words cost 12 of the
+// instruction's 28 L1 cycles).  Groups of SRV_GROUP independent
+// instructions keep 3 * SRV_GROUP shared loads in flight, and the records of
+// the next group are loaded while the current one computes.
 //
 // Scheduling is on the device: every warp starts at its own job of the epoch
 // table and claims tiles of that job's slice with an atomic cursor, moving on
@@ -25,6 +35,13 @@ typedef unsigned long long u64;
 
 namespace {
 
+constexpr int W = SRV_WORDS;
+constexpr int G = SRV_GROUP;
+constexpr int LOGW = SRV_LOG_WORDS;
+constexpr u32 ITERS = 32u / W;                 // program passes per tile
+static_assert(W == 2 || W == 4, "SRV_WORDS must be 2 or 4");
+static_assert((1 << LOGW) == W, "SRV_LOG_WORDS");
+
 template <int LUT>
 __device__ __forceinline__ u32 lop3(u32 a, u32 b, u32 c) {
     u32 d;
@@ -34,15 +51,6 @@ __device__ __forceinline__ u32 lop3(u32 a, u32 b, u32 c) {
 
 // s ? x1 : x0, bitwise
 __device__ __forceinline__ u32 mux(u32 s, u32 x1, u32 x0) { return lop3<0xCA>(s, x1, x0); }
-
-// 3-input LUT with a runtime truth table (row = a<<2 | b<<1 | c)
-__device__ __forceinline__ u32 lut3(u32 a, u32 b, u32 c, u32 tt) {
-    const u32 t0 = 0u - (tt & 1u), t1 = 0u - ((tt >> 1) & 1u), t2 = 0u - ((tt >> 2) & 1u),
-              t3 = 0u - ((tt >> 3) & 1u), t4 = 0u - ((tt >> 4) & 1u), t5 = 0u - ((tt >> 5) & 1u),
-              t6 = 0u - ((tt >> 6) & 1u), t7 = 0u - ((tt >> 7) & 1u);
-    const u32 x01 = mux(c, t1, t0), x23 = mux(c, t3, t2), x45 = mux(c, t5, t4), x67 = mux(c, t7, t6);
-    return mux(a, mux(b, x67, x45), mux(b, x23, x01));
-}
 
 __device__ __forceinline__ u64 warp_min(u64 v) {
 #pragma unroll
@@ -82,105 +90,198 @@ __device__ __forceinline__ void transpose32(u32* a) {
     }
 }
 
-// Runs a job's program on one word per lane; slots S[slot * 32 + lane].
-__device__ __forceinline__ void run_program(const srv_u64* __restrict__ prog, u32 ninstr,
-                                            u32* __restrict__ S, u32 lane) {
-    u32 i = 0;
-    for (; i + 2 <= ninstr; i += 2) {
-        const u64 p0 = __ldg(prog + i), p1 = __ldg(prog + i + 1);
-        const u32 a0 = S[((u32)p0 & 0xfffu) * 32 + lane], b0 = S[((u32)(p0 >> 12) & 0xfffu) * 32 + lane],
-                  c0 = S[((u32)(p0 >> 24) & 0xfffu) * 32 + lane];
-        S[((u32)(p0 >> 36) & 0xfffu) * 32 + lane] = lut3(a0, b0, c0, (u32)(p0 >> 48) & 0xffu);
-        const u32 a1 = S[((u32)p1 & 0xfffu) * 32 + lane], b1 = S[((u32)(p1 >> 12) & 0xfffu) * 32 + lane],
-                  c1 = S[((u32)(p1 >> 24) & 0xfffu) * 32 + lane];
-        S[((u32)(p1 >> 36) & 0xfffu) * 32 + lane] = lut3(a1, b1, c1, (u32)(p1 >> 48) & 0xffu);
+struct Vals {
+    u32 v[W];
+};
+
+__device__ __forceinline__ Vals lds(const char* p) {
+    Vals r;
+    if constexpr (W == 4) {
+        const uint4 t = *reinterpret_cast<const uint4*>(p);
+        r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+    } else {
+        const uint2 t = *reinterpret_cast<const uint2*>(p);
+        r.v[0] = t.x; r.v[1] = t.y;
     }
-    if (i < ninstr) {
-        const u64 p0 = __ldg(prog + i);
-        const u32 a0 = S[((u32)p0 & 0xfffu) * 32 + lane], b0 = S[((u32)(p0 >> 12) & 0xfffu) * 32 + lane],
-                  c0 = S[((u32)(p0 >> 24) & 0xfffu) * 32 + lane];
-        S[((u32)(p0 >> 36) & 0xfffu) * 32 + lane] = lut3(a0, b0, c0, (u32)(p0 >> 48) & 0xffu);
+    return r;
+}
+
+__device__ __forceinline__ void sts(char* p, const Vals& x) {
+    if constexpr (W == 4) *reinterpret_cast<uint4*>(p) = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    else *reinterpret_cast<uint2*>(p) = make_uint2(x.v[0], x.v[1]);
+}
+
+// Mask k of a spread truth table: byte k of {thi, tlo} with its sign bit
+// replicated over all 32 bits (prmt in its default mode: a selector nibble
+// with bit 3 set replicates the sign of the byte its low 3 bits select; the
+// __byte_perm intrinsic is only defined for the low 3 bits).
+template <int K>
+__device__ __forceinline__ u32 tt_mask(u32 tlo, u32 thi) {
+    u32 d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(tlo), "r"(thi), "n"((8 | K) * 0x1111));
+    return d;
+}
+
+struct Lut {
+    u32 m0, m1, m2, m3, m4, m5, m6, m7;
+};
+
+__device__ __forceinline__ Lut expand(const uint4& r) {
+    Lut t;
+    t.m0 = tt_mask<0>(r.z, r.w); t.m1 = tt_mask<1>(r.z, r.w); t.m2 = tt_mask<2>(r.z, r.w); t.m3 = tt_mask<3>(r.z, r.w);
+    t.m4 = tt_mask<4>(r.z, r.w); t.m5 = tt_mask<5>(r.z, r.w); t.m6 = tt_mask<6>(r.z, r.w); t.m7 = tt_mask<7>(r.z, r.w);
+    return t;
+}
+
+// LUT through a mux tree over the truth-table masks (7 lop3)
+__device__ __forceinline__ u32 lut_mux(u32 a, u32 b, u32 c, const Lut& t) {
+    const u32 x01 = mux(c, t.m1, t.m0), x23 = mux(c, t.m3, t.m2), x45 = mux(c, t.m5, t.m4), x67 = mux(c, t.m7, t.m6);
+    return mux(a, mux(b, x67, x45), mux(b, x23, x01));
+}
+
+__device__ __forceinline__ u32 slot_off(u32 s) { return s * SRV_SLOT_BYTES; }
+
+// Runs a job's program once on this lane's W words.  Sl is the warp's slot
+// area plus lane * W * 4.
+__device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32 ngroups, char* __restrict__ Sl) {
+    if (ngroups == 0) return;
+    const uint4* P = reinterpret_cast<const uint4*>(prog);
+    uint4 cur[G];
+#pragma unroll
+    for (int k = 0; k < G; k++) cur[k] = __ldg(P + k);
+    for (u32 g = 0; g < ngroups; g++) {
+        Vals a[G], b[G], c[G];
+#pragma unroll
+        for (int k = 0; k < G; k++) {
+            a[k] = lds(Sl + slot_off(cur[k].x & 0xffffu));
+            b[k] = lds(Sl + slot_off(cur[k].x >> 16));
+            c[k] = lds(Sl + slot_off(cur[k].y & 0xffffu));
+        }
+        // records of the next group (the last group re-reads itself)
+        const uint4* nx = P + (size_t)(g + 1 < ngroups ? g + 1 : g) * G;
+        uint4 nxt[G];
+#pragma unroll
+        for (int k = 0; k < G; k++) nxt[k] = __ldg(nx + k);
+#pragma unroll
+        for (int k = 0; k < G; k++) {
+            const Lut t = expand(cur[k]);
+            Vals d;
+#pragma unroll
+            for (int w = 0; w < W; w++) d.v[w] = lut_mux(a[k].v[w], b[k].v[w], c[k].v[w], t);
+            sts(Sl + slot_off(cur[k].y >> 16), d);
+        }
+#pragma unroll
+        for (int k = 0; k < G; k++) cur[k] = nxt[k];
     }
 }
 
-__device__ __forceinline__ u32 read_out(const u32* S, const uint16_t* outs, u32 j, u32 lane) {
+__device__ __forceinline__ Vals read_out(const char* Sl, const uint16_t* outs, u32 j) {
     const uint16_t o = __ldg(outs + j);
-    const u32 v = S[(o & 0x7fffu) * 32 + lane];
-    return (o & 0x8000u) ? ~v : v;
+    Vals v = lds(Sl + (u32)(o & 0x7fffu) * SRV_SLOT_BYTES);
+    if (o & 0x8000u) {
+#pragma unroll
+        for (int w = 0; w < W; w++) v.v[w] = ~v.v[w];
+    }
+    return v;
+}
+
+// Enumeration inside a tile: bits 0-4 the bit of a word, 5-9 the lane,
+// 10 .. 10+LOGW-1 which of the lane's words, the rest up to bit 14 the pass;
+// bits from SRV_TILE_BITS up are the tile index.  Input slots are rewritten
+// every pass because the program reuses slots of inputs it has finished
+// reading.
+__device__ __forceinline__ void set_inputs(const SrvJob* J, u64 tile_base, u32 it, u32 lane, char* Sl) {
+    const u32 nb = J->nb < SRV_MAX_NB ? J->nb : SRV_MAX_NB;
+    for (u32 p = 0; p < nb; p++) {
+        const int s = J->in_slot[p];
+        if (s < 0) continue;
+        Vals v;
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            u32 x;
+            if (p < 5) x = p == 0 ? 0xAAAAAAAAu : p == 1 ? 0xCCCCCCCCu : p == 2 ? 0xF0F0F0F0u : p == 3 ? 0xFF00FF00u : 0xFFFF0000u;
+            else if (p < 10) x = 0u - ((lane >> (p - 5)) & 1u);
+            else if (p < 10 + LOGW) x = 0u - (((u32)w >> (p - 10)) & 1u);
+            else if (p < SRV_TILE_BITS) x = 0u - ((it >> (p - 10 - LOGW)) & 1u);
+            else x = 0u - (u32)((tile_base >> p) & 1ull);
+            v.v[w] = x;
+        }
+        sts(Sl + (u32)s * SRV_SLOT_BYTES, v);
+    }
 }
 
 // Evaluates tile `tile` of job `J` with this warp.
-__device__ void do_tile(SrvJob* J, u64 tile, u32* __restrict__ S, u32 lane, uint8_t* __restrict__ vals) {
-    const u32 nb = J->nb;
+__device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ Sl, u32 lane, uint8_t* __restrict__ vals) {
     const u64 tile_base = tile << SRV_TILE_BITS;     // first assignment of the tile
-    // inputs fixed for the tile: word lanes, warp lanes, tile bits
-    for (u32 p = 0; p < nb && p < SRV_MAX_NB; p++) {
-        const int s = J->in_slot[p];
-        if (s < 0 || (p >= 10 && p < 15)) continue;
-        u32 v;
-        if (p < 5) v = p == 0 ? 0xAAAAAAAAu : p == 1 ? 0xCCCCCCCCu : p == 2 ? 0xF0F0F0F0u : p == 3 ? 0xFF00FF00u : 0xFFFF0000u;
-        else if (p < 10) v = 0u - ((lane >> (p - 5)) & 1u);
-        else v = 0u - (u32)((tile_base >> p) & 1ull);
-        S[s * 32 + lane] = v;
-    }
-    __syncwarp();
     const u32 kind = J->kind;
-    u32 cnt = 0, first_it = 0xffffffffu, first_bit = 0;
+    const SrvIns* prog = J->prog;
+    const u32 ngroups = J->ngroups;
+    u32 cnt = 0, first = 0xffffffffu;   // SAT: first (row, bit) with a solution, row = it * W + word
     u64 cand = ~0ull;
     u32 acc = 0;
     const u32 M = J->m;
     const u64 allbits = J->allbits;
     const u32 dec_all = J->q0all;
-    for (u32 it = 0; it < 32; it++) {
-        for (u32 p = 10; p < 15 && p < nb; p++) {
-            const int s = J->in_slot[p];
-            if (s >= 0) S[s * 32 + lane] = 0u - ((it >> (p - 10)) & 1u);
-        }
-        __syncwarp();
-        run_program(J->prog, J->ninstr, S, lane);
-        __syncwarp();
+    for (u32 it = 0; it < ITERS; it++) {
+        set_inputs(J, tile_base, it, lane, Sl);
+        run_program(prog, ngroups, Sl);
         if (kind == SRV_SAT) {
-            const u32 y = read_out(S, J->outs, 0, lane);
-            cnt += __popc(y);
-            if (y != 0u && first_it == 0xffffffffu) { first_it = it; first_bit = __ffs(y) - 1; }
-        } else if (kind == SRV_QSAT) {
-            u32 y = read_out(S, J->outs, 0, lane);
-            const u64 wbase = tile_base + ((u64)it << 10);      // first item of this warp iteration
-            if (M < 5) {
-                y = tree_rt(y, allbits, 0, (int)M);
-                const u32 d = (dec_all ? ~y : y) & unit_mask((int)M);
-                if (d != 0u && cand == ~0ull) cand = ((wbase + ((u64)lane << 5)) >> M) + ((__ffs(d) - 1) >> M);
-                continue;
-            }
-            y = tree_rt(y, allbits, 0, 5);
-            u32 b = __ballot_sync(0xffffffffu, y & 1u);
-            if (M < 10) {
-                b = tree_rt(b, allbits, 5, (int)M - 5);
-                const u32 d = (dec_all ? ~b : b) & unit_mask((int)M - 5);
-                if (d != 0u && cand == ~0ull) cand = (wbase >> M) + ((__ffs(d) - 1) >> (M - 5));
-                continue;
-            }
-            b = tree_rt(b, allbits, 5, 5);
-            acc |= (b & 1u) << it;
-        } else {   // SRV_TABLE
-            u32 o[32];
+            const Vals y = read_out(Sl, J->outs, 0);
 #pragma unroll
-            for (int k = 0; k < 32; k++) o[k] = (u32)k < J->nout ? read_out(S, J->outs, k, lane) : 0u;
-            transpose32(o);
-            const u64 w = (tile_base >> 5) + ((u64)it << 5) + lane;   // word index
+            for (int w = 0; w < W; w++) {
+                cnt += __popc(y.v[w]);
+                if (first == 0xffffffffu && y.v[w]) first = ((it * W + w) << 5) | (u32)(__ffs(y.v[w]) - 1);
+            }
+        } else if (kind == SRV_QSAT) {
+            const Vals yy = read_out(Sl, J->outs, 0);
+#pragma unroll
+            for (int w = 0; w < W; w++) {
+                u32 y = yy.v[w];
+                const u32 row = it * W + w;
+                const u64 wbase = tile_base + ((u64)row << 10);   // first item of this word row
+                if (M < 5) {
+                    y = tree_rt(y, allbits, 0, (int)M);
+                    const u32 d = (dec_all ? ~y : y) & unit_mask((int)M);
+                    if (d != 0u && cand == ~0ull) cand = ((wbase + ((u64)lane << 5)) >> M) + ((__ffs(d) - 1) >> M);
+                    continue;
+                }
+                y = tree_rt(y, allbits, 0, 5);
+                u32 b = __ballot_sync(0xffffffffu, y & 1u);
+                if (M < 10) {
+                    b = tree_rt(b, allbits, 5, (int)M - 5);
+                    const u32 d = (dec_all ? ~b : b) & unit_mask((int)M - 5);
+                    if (d != 0u && cand == ~0ull) cand = (wbase >> M) + ((__ffs(d) - 1) >> (M - 5));
+                    continue;
+                }
+                b = tree_rt(b, allbits, 5, 5);
+                acc |= (b & 1u) << row;
+            }
+        } else {   // SRV_TABLE
             const u32 lanes = J->n >= 5 ? 32u : (1u << J->n);
             const u64 states = 1ull << J->n;
-            if ((w << 5) < states) {
-                u64* dst = J->table + (w << 5);
-                for (u32 l = 0; l < lanes; l++) dst[l] = (u64)o[l] | (1ull << 32);
+            const u32 nout = J->nout;
+            u32 stop_any = 0;
+            for (int w = 0; w < W; w++) {
+                u32 o[32];
+#pragma unroll
+                for (int k = 0; k < 32; k++) {
+                    if ((u32)k < nout) o[k] = read_out(Sl, J->outs, k).v[w];
+                    else o[k] = 0u;
+                }
+                stop_any |= o[nout - 1];
+                transpose32(o);
+                const u64 word = (tile_base >> 5) + ((u64)(it * W + w) << 5) + lane;   // word index
+                if ((word << 5) < states) {
+                    srv_u64* dst = J->table + (word << 5);
+                    for (u32 l = 0; l < lanes; l++) dst[l] = (srv_u64)o[l] | (1ull << 32);
+                }
             }
-            const u32 stop = read_out(S, J->outs, J->nout - 1, lane);
-            if (__any_sync(0xffffffffu, stop != 0u) && lane == 0) atomicOr(&J->any, 1u);
+            if (__any_sync(0xffffffffu, stop_any != 0u) && lane == 0) atomicOr(&J->any, 1u);
         }
     }
     if (kind == SRV_SAT) {
         u64 idx = ~0ull;
-        if (first_it != 0xffffffffu) idx = tile_base + ((u64)first_it << 10) + ((u64)lane << 5) + first_bit;
+        if (first != 0xffffffffu) idx = tile_base + ((u64)(first >> 5) << 10) + ((u64)lane << 5) + (first & 31u);
         idx = warp_min(idx);
         cnt = __reduce_add_sync(0xffffffffu, cnt);
         if (lane == 0 && cnt) {
@@ -203,15 +304,14 @@ __device__ void do_tile(SrvJob* J, u64 tile, u32* __restrict__ S, u32 lane, uint
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(SRV_WARPS_PER_CTA * 32) serve_epoch(const SrvEpoch* __restrict__ hdr, SrvJob* __restrict__ jobs,
-                                                   u32 max_slots, uint8_t* __restrict__ vals) {
-    extern __shared__ u32 smem[];
+// One warp per CTA; the dynamic shared memory is max_slots * SRV_SLOT_BYTES.
+__global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict__ hdr, SrvJob* __restrict__ jobs,
+                                                  uint8_t* __restrict__ vals) {
+    extern __shared__ __align__(16) char smem[];
     const u32 njobs = hdr->njobs;
     const u32 lane = threadIdx.x & 31u;
-    const u32 wid = threadIdx.x >> 5;
-    u32* S = smem + (size_t)wid * max_slots * 32;
-    const u32 gw = blockIdx.x * (blockDim.x >> 5) + wid;
-    u32 j = njobs ? gw % njobs : 0;
+    char* Sl = smem + lane * (W * 4);
+    u32 j = njobs ? blockIdx.x % njobs : 0;
     u32 dry = 0;     // consecutive jobs found exhausted
     while (dry < njobs) {
         SrvJob* J = jobs + j;
@@ -224,7 +324,7 @@ __global__ void __launch_bounds__(SRV_WARPS_PER_CTA * 32) serve_epoch(const SrvE
             continue;
         }
         dry = 0;
-        do_tile(J, tile, S, lane, vals);
+        do_tile(J, tile, Sl, lane, vals);
     }
 }
 
@@ -233,15 +333,15 @@ __global__ void __launch_bounds__(SRV_WARPS_PER_CTA * 32) serve_epoch(const SrvE
 extern "C" int nsat_launch_serve_epoch(const SrvEpoch* hdr, SrvJob* jobs, uint32_t max_slots, uint8_t* vals,
                                        int grid, cudaStream_t stream) {
     // the dynamic shared memory limit was raised by nsat_serve_occupancy
-    const size_t smem = (size_t)SRV_WARPS_PER_CTA * max_slots * 32 * sizeof(u32);
-    serve_epoch<<<grid, SRV_WARPS_PER_CTA * 32, smem, stream>>>(hdr, jobs, max_slots, vals);
+    const size_t smem = (size_t)max_slots * SRV_SLOT_BYTES;
+    serve_epoch<<<grid, 32, smem, stream>>>(hdr, jobs, vals);
     return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 
 extern "C" int nsat_serve_occupancy(uint32_t max_slots, int* ctas_per_sm) {
-    const size_t smem = (size_t)SRV_WARPS_PER_CTA * max_slots * 32 * sizeof(u32);
-    if (cudaFuncSetAttribute(serve_epoch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    const size_t smem = (size_t)max_slots * SRV_SLOT_BYTES;
+    const void* fn = (const void*)serve_epoch;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -4;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, serve_epoch, SRV_WARPS_PER_CTA * 32, smem) ==
-                   cudaSuccess ? 0 : -4;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32, smem) == cudaSuccess ? 0 : -4;
 }

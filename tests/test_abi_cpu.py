@@ -117,3 +117,23 @@ def test_library_lfsr_generator_matches_python(seed, n, g):
     a = W.lfsr_stop(seed, n, g)
     b = W.lfsr_stop_py(seed, n, g)
     assert (a.gates == b.gates).all() and (a.outputs == b.outputs).all() and a.pattern == b.pattern
+
+
+@pytest.mark.parametrize("seed,n,g", [(1, 34, 4000), (2, 30, 1000), (3, 20, 100), (4, 26, 600), (9, 18, 60),
+                                      (11, 22, 2500)])
+def test_server_program_matches_circuit(seed, n, g):
+    """The interpreter program (groups of independent LUTs, recycled slots)
+    computes the circuit's output on random assignments."""
+    c = W.random_dag(seed, n, g, output="live")
+    slots, luts, nops = api.server_program_check(c, "sat", seed=seed)
+    assert luts > 0 and slots <= 384
+    assert nops <= luts // 4 + 8
+
+
+def test_server_program_check_on_config_circuits():
+    for name, kind in [("c0", "sat"), ("c1", "sat"), ("c2a", "qsat"), ("c2c", "qsat"), ("c3a", "stop"),
+                       ("c3b", "stop")]:
+        api.server_program_check(W.config(name), kind)
+    for r in W.serving_requests(60, seed=3, rate_hz=1e9, n_range=(12, 22), g_range=(40, 900),
+                                stop_n_range=(8, 14)):
+        api.server_program_check(r["circ"], r["kind"], seed=5)

@@ -59,13 +59,29 @@ def test_mixed_batch_matches_oracle_and_alone(ctx):
         alone.close()
 
 
+def test_find_all_counts_every_solution(ctx):
+    reqs = [r for r in small_mix(40, 31) if r["kind"] == "sat"][:12]
+    srv = api.Server(ctx)
+    for i, r in enumerate(reqs):
+        srv.submit("sat", r["circ"], tag=i, find_all=True)
+    res = {r["tag"]: r for r in srv.run_all()}
+    for i, r in enumerate(reqs):
+        c = r["circ"]
+        cnt, low = O.sat_range(O.Circuit(c.n, c.gates, c.outputs))
+        assert (res[i]["count"], res[i]["satisfiable"], res[i]["witness"]) == (cnt, low is not None, low), i
+
+
 def test_large_jobs_match_one_shot_solvers(ctx):
     """n = 26..30 jobs against the compiled one-shot solvers (the oracle would
     be slow here); slices span many epochs."""
     reqs = W.serving_requests(6, seed=5, rate_hz=1e9, n_range=(26, 30), g_range=(200, 1200), mix=(0.5, 0.5, 0.0))
     srv = api.Server(ctx)
     submit_all(srv, reqs)
+    sat0 = next(i for i, r in enumerate(reqs) if r["kind"] == "sat")
+    srv.submit("sat", reqs[sat0]["circ"], tag=100, find_all=True)
     res = {r["tag"]: r for r in srv.run_all()}
+    full = ctx.circuit(reqs[sat0]["circ"]).sat(find_all=True)
+    assert (res[100]["count"], res[100]["witness"]) == (full["count"], full["witness"])
     for i, r in enumerate(reqs):
         h = ctx.circuit(r["circ"])
         if r["kind"] == "sat":
