@@ -270,6 +270,7 @@ typedef struct {
     uint32_t active, queued;
     uint64_t arena_used, arena_bytes;
     uint32_t graph_slots, grid;
+    uint64_t launches;          /* kernels launched: epoch graphs and join rounds */
 } nsat_server_stats_t;
 
 int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out);

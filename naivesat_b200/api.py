@@ -102,7 +102,7 @@ class JobResult(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("epochs", C.c_uint64), ("device_ms", C.c_double), ("active", C.c_uint32),
                 ("queued", C.c_uint32), ("arena_used", C.c_uint64), ("arena_bytes", C.c_uint64),
-                ("graph_slots", C.c_uint32), ("grid", C.c_uint32)]
+                ("graph_slots", C.c_uint32), ("grid", C.c_uint32), ("launches", C.c_uint64)]
 
 
 EXPORTS = [
@@ -274,10 +274,13 @@ class CircuitHandle:
         ctx._check(lib().nsat_circuit_new(ctx.h, C.byref(d), C.byref(h)), "circuit_new")
         self.h = h
 
-    def __del__(self):
+    def close(self):
         if getattr(self, "h", None):
             lib().nsat_circuit_free(self.h)
             self.h = None
+
+    def __del__(self):
+        self.close()
 
     def stats(self, output=0):
         live, ops = C.c_uint32(), C.c_uint32()

@@ -212,7 +212,11 @@ struct Job {
     Program prog;
     uint32_t n = 0, nb = 0, d = 0;   // inputs, enumeration bits, dummy bits
     uint32_t f = 0, m = 0;           // QSAT first block length, unit level
-    uint64_t total_tiles = 0, cursor = 0, slice = 1;
+    uint64_t total_tiles = 0;
+    uint64_t cursor = 0;             // tiles whose results were processed
+    uint64_t sched = 0;              // tiles handed to launched epochs
+    uint64_t slice = 1;
+    uint32_t inflight = 0;           // launched epochs holding a slice whose results are not processed yet
     std::unique_ptr<QuantReducer> qr;
     SrvJob rec{};
     size_t prog_off = 0, outs_off = 0, table_off = 0, table2_off = 0, reserve = 0;
@@ -221,6 +225,24 @@ struct Job {
     bool finished = false;
     uint64_t count = 0;
     nsat_job_result res{};
+};
+
+// One of the two epoch buffers: while the device runs the epoch of one, the
+// host reads the results of the other and fills it again.
+struct EpochBuf {
+    SrvEpoch* d_hdr = nullptr;
+    SrvJob* d_jobs = nullptr;
+    uint8_t* d_vals = nullptr;
+    SrvEpoch* h_hdr = nullptr;
+    SrvJob* h_jobs = nullptr;
+    uint8_t* h_vals = nullptr;
+    // epoch graphs by (narrow slots, wide slots; 0 = no wide launch)
+    std::map<std::pair<uint32_t, uint32_t>, cudaGraphExec_t> graphs;
+    uint32_t max_slots = 0;
+    int grid = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<Job*> jobs;          // the launched epoch's jobs, in table order
+    bool launched = false;
 };
 
 }  // namespace
@@ -234,36 +256,36 @@ struct nsat_server {
     std::vector<nsat_job_result> done;
     uint64_t next_id = 1;
     uint32_t rr = 0;   // rotating start of the epoch table
-    SrvEpoch* d_hdr = nullptr;
-    SrvJob* d_jobs = nullptr;
-    uint8_t* d_vals = nullptr;
-    SrvEpoch* h_hdr = nullptr;
-    SrvJob* h_jobs = nullptr;
-    uint8_t* h_vals = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    uint32_t graph_slots = 0;
-    int grid = 0;
+    EpochBuf buf[2];
+    int cur = 0;       // buffer the next epoch is built in
+    cudaStream_t cap = nullptr, cap2 = nullptr;   // streams the epoch graphs are captured on (never run work)
+    cudaEvent_t fork = nullptr, join = nullptr;
     NsatJoinState* d_join = nullptr;
     NsatJoinState* h_join = nullptr;
-    uint64_t epochs = 0;
+    uint64_t epochs = 0, launches = 0;
     double device_ms = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     ~nsat_server() {
         cudaSetDevice(ctx_device(ctx));
         cudaStreamSynchronize(ctx_stream(ctx));
-        if (graph) cudaGraphExecDestroy(graph);
+        for (EpochBuf& b : buf) {
+            for (auto& kv : b.graphs) cudaGraphExecDestroy(kv.second);
+            cudaFree(b.d_hdr);
+            cudaFree(b.d_jobs);
+            cudaFree(b.d_vals);
+            cudaFreeHost(b.h_hdr);
+            cudaFreeHost(b.h_jobs);
+            cudaFreeHost(b.h_vals);
+            if (b.ev0) cudaEventDestroy(b.ev0);
+            if (b.ev1) cudaEventDestroy(b.ev1);
+        }
+        if (cap) cudaStreamDestroy(cap);
+        if (cap2) cudaStreamDestroy(cap2);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
         cudaFree(arena.base);
-        cudaFree(d_hdr);
-        cudaFree(d_jobs);
-        cudaFree(d_vals);
         cudaFree(d_join);
-        cudaFreeHost(h_hdr);
-        cudaFreeHost(h_jobs);
-        cudaFreeHost(h_vals);
         cudaFreeHost(h_join);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
     }
 };
 
@@ -277,29 +299,41 @@ namespace {
                             std::string(#call) + ": " + cudaGetErrorString(e_));                    \
     } while (0)
 
-int capture_graph(nsat_server* s, uint32_t slots) {
-    cudaStream_t st = ctx_stream(s->ctx);
-    int per_sm = 0;
-    if (nsat_serve_occupancy(slots, &per_sm) || per_sm < 1)
-        return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, "interpreter does not fit with " + std::to_string(slots) + " slots");
-    s->grid = per_sm * ctx_sm_count(s->ctx);
-    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+// Captures buffer b's epoch graph for (narrow, wide) slots per warp: H2D of
+// the table; the narrow launch and, when wide > 0, the wide launch as
+// parallel branches; D2H of the table and the QSAT tile values.
+int capture_graph(nsat_server* s, EpochBuf& b, uint32_t narrow, uint32_t wide, cudaGraphExec_t* out) {
+    int per_sm[2] = {0, 0};
+    const uint32_t slots[2] = {narrow, wide};
+    for (int c = 0; c < (wide ? 2 : 1); c++)
+        if (nsat_serve_occupancy(slots[c], &per_sm[c]) || per_sm[c] < 1)
+            return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, "interpreter does not fit with " + std::to_string(slots[c]) + " slots");
+    b.grid = per_sm[0] * ctx_sm_count(s->ctx);
     cudaGraph_t g = nullptr;
+    cudaStream_t st = s->cap;
     SCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    cudaMemcpyAsync(s->d_hdr, s->h_hdr, sizeof(SrvEpoch), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s->d_jobs, s->h_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyHostToDevice, st);
-    int rc = nsat_launch_serve_epoch(s->d_hdr, s->d_jobs, slots, s->d_vals, s->grid, st);
-    cudaMemcpyAsync(s->h_jobs, s->d_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(s->h_vals, s->d_vals, kValsCap, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(b.d_hdr, b.h_hdr, sizeof(SrvEpoch), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(b.d_jobs, b.h_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyHostToDevice, st);
+    int rc = 0;
+    if (wide) {
+        cudaEventRecord(s->fork, st);
+        cudaStreamWaitEvent(s->cap2, s->fork, 0);
+        rc |= nsat_launch_serve_epoch(b.d_hdr, b.d_jobs, wide, b.d_vals, per_sm[1] * ctx_sm_count(s->ctx), 1, s->cap2);
+        cudaEventRecord(s->join, s->cap2);
+    }
+    rc |= nsat_launch_serve_epoch(b.d_hdr, b.d_jobs, narrow, b.d_vals, b.grid, 0, st);
+    if (wide) cudaStreamWaitEvent(st, s->join, 0);
+    cudaMemcpyAsync(b.h_jobs, b.d_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(b.h_vals, b.d_vals, kValsCap, cudaMemcpyDeviceToHost, st);
     cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (rc || ce != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
         return ctx_fail(s->ctx, NSAT_ECUDA, "epoch graph capture failed");
     }
-    cudaError_t ie = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaError_t ie = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) return ctx_fail(s->ctx, NSAT_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
-    s->graph_slots = slots;
+    b.max_slots = std::max(b.max_slots, std::max(narrow, wide));
     return NSAT_OK;
 }
 
@@ -328,6 +362,7 @@ int admit(nsat_server* s, Job* j) {
     j->table_off = offs[2]; j->table2_off = offs[3];
     j->reserve = pbytes + obytes + 2 * tbytes;
     cudaStream_t st = ctx_stream(s->ctx);
+    // ordered before every epoch that reads them (same stream)
     SCK(cudaMemcpyAsync(s->arena.base + j->prog_off, j->prog.ins.data(), j->prog.ins.size() * sizeof(SrvIns),
                         cudaMemcpyHostToDevice, st));
     SCK(cudaMemcpyAsync(s->arena.base + j->outs_off, j->prog.outs.data(), j->prog.outs.size() * 2, cudaMemcpyHostToDevice, st));
@@ -388,6 +423,7 @@ int run_joins(nsat_server* s, Job* j) {
         if (nsat_launch_join_round(2, buf[src], buf[src ^ 1], 1ull << j->n, j->n, j->unknowns, r, 1, s->d_join,
                                    ctx_sm_count(s->ctx), st))
             return ctx_fail(s->ctx, NSAT_ECUDA, "join launch failed");
+        s->launches++;
         src ^= 1;
     }
     SCK(cudaMemcpyAsync(h, s->d_join, sizeof(*h), cudaMemcpyDeviceToHost, st));
@@ -424,18 +460,24 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     SCK(cudaMalloc(&s->arena.base, s->opts.arena_bytes));
     s->arena.cap = s->opts.arena_bytes;
     s->arena.free_[0] = s->opts.arena_bytes;
-    SCK(cudaMalloc(&s->d_hdr, sizeof(SrvEpoch)));
-    SCK(cudaMalloc(&s->d_jobs, sizeof(SrvJob) * kMaxActive));
-    SCK(cudaMalloc(&s->d_vals, kValsCap));
+    for (EpochBuf& b : s->buf) {
+        SCK(cudaMalloc(&b.d_hdr, sizeof(SrvEpoch)));
+        SCK(cudaMalloc(&b.d_jobs, sizeof(SrvJob) * kMaxActive));
+        SCK(cudaMalloc(&b.d_vals, kValsCap));
+        SCK(cudaMallocHost(&b.h_hdr, sizeof(SrvEpoch)));
+        SCK(cudaMallocHost(&b.h_jobs, sizeof(SrvJob) * kMaxActive));
+        SCK(cudaMallocHost(&b.h_vals, kValsCap));
+        memset(b.h_hdr, 0, sizeof(SrvEpoch));
+        memset(b.h_jobs, 0, sizeof(SrvJob) * kMaxActive);
+        SCK(cudaEventCreate(&b.ev0));
+        SCK(cudaEventCreate(&b.ev1));
+    }
+    SCK(cudaStreamCreateWithFlags(&s->cap, cudaStreamNonBlocking));
+    SCK(cudaStreamCreateWithFlags(&s->cap2, cudaStreamNonBlocking));
+    SCK(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
+    SCK(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
     SCK(cudaMalloc(&s->d_join, sizeof(NsatJoinState)));
-    SCK(cudaMallocHost(&s->h_hdr, sizeof(SrvEpoch)));
-    SCK(cudaMallocHost(&s->h_jobs, sizeof(SrvJob) * kMaxActive));
-    SCK(cudaMallocHost(&s->h_vals, kValsCap));
     SCK(cudaMallocHost(&s->h_join, sizeof(NsatJoinState)));
-    memset(s->h_hdr, 0, sizeof(SrvEpoch));
-    memset(s->h_jobs, 0, sizeof(SrvJob) * kMaxActive);
-    SCK(cudaEventCreate(&s->ev0));
-    SCK(cudaEventCreate(&s->ev1));
     *out = sp.release();
     return NSAT_OK;
 }
@@ -506,39 +548,29 @@ extern "C" int nsat_server_submit(nsat_server* s, const nsat_job_desc* jd, uint6
     return NSAT_OK;
 }
 
-extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_queued) {
-    if (!s) return NSAT_EINVAL;
-    SCK(cudaSetDevice(ctx_device(s->ctx)));
-    // admission in arrival order, by device memory
-    while (!s->queue.empty() && s->active.size() < s->opts.max_active) {
-        Job* j = s->queue.front().get();
-        int a = admit(s, j);
-        if (a < 0) return a;
-        if (a > 0) break;   // does not fit yet
-        s->active.push_back(std::move(s->queue.front()));
-        s->queue.pop_front();
-    }
-    if (s->active.empty()) {
-        if (n_active) *n_active = 0;
-        if (n_queued) *n_queued = (uint32_t)s->queue.size();
-        return NSAT_OK;
-    }
-    // epoch table: slices of every active job, within the work budget
+namespace {
+
+// Fills buffer b with slices of the active jobs (within the work budget) and
+// launches its epoch graph.  Slices start where the previous launched slice
+// ended, so a job may get a slice while its previous one is still running.
+int launch_epoch(nsat_server* s, EpochBuf& b) {
     const uint32_t na = (uint32_t)s->active.size();
     uint64_t budget = s->opts.epoch_budget;
     size_t vals = 0;
-    uint32_t k = 0, slots = 16;
-    std::vector<Job*> in_epoch;
+    uint32_t k = 0, narrow = 32, wide = 0;
+    std::vector<Job*> sel[2];
+    std::vector<SrvJob> recs[2];
     for (uint32_t t = 0; t < na; t++) {
         Job* j = s->active[(s->rr + t) % na].get();
-        uint64_t want = std::min<uint64_t>(j->slice, j->total_tiles - j->cursor);
+        if (j->finished) continue;
+        uint64_t want = std::min<uint64_t>(j->slice, j->total_tiles - j->sched);
         const uint64_t cost_per_tile = std::max<uint64_t>(1, j->prog.ins.size());
         if (k > 0 && want * cost_per_tile > budget) want = budget / cost_per_tile;
         if (j->kind == SRV_QSAT && j->qr) want = std::min<uint64_t>(want, kValsCap - vals);
         if (want == 0) continue;
         SrvJob& r = j->rec;
-        r.tile_begin = j->cursor;
-        r.tile_end = j->cursor + want;
+        r.tile_begin = j->sched;
+        r.tile_end = j->sched + want;
         r.claim = r.tile_begin;
         r.count = 0;
         r.min_idx = ~0ull;
@@ -546,44 +578,75 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
         r.val_off = (uint32_t)vals;
         if (j->kind == SRV_QSAT && j->qr) vals += want;
         budget -= std::min<uint64_t>(budget, want * cost_per_tile);
-        s->h_jobs[k++] = r;
-        slots = std::max<uint32_t>(slots, (j->prog.nslots + 15) & ~15u);
-        in_epoch.push_back(j);
+        k++;
+        const uint32_t sl = (j->prog.nslots + 15) & ~15u;
+        const int c = sl > SRV_NARROW_SLOTS ? 1 : 0;
+        if (c) wide = std::max(wide, sl);
+        else narrow = std::max(narrow, sl);
+        sel[c].push_back(j);
+        recs[c].push_back(r);
+        j->sched += want;
+        j->slice = std::min<uint64_t>(j->slice * 2, s->opts.max_slice_tiles);
+        j->inflight++;
     }
-    s->rr = (s->rr + 1) % na;
-    s->h_hdr->njobs = k;
-    if (!s->graph || slots > s->graph_slots) {
-        if (int rc = capture_graph(s, std::max(slots, s->graph_slots))) return rc;
+    if (na) s->rr = (s->rr + 1) % na;
+    b.jobs.clear();
+    if (k == 0) return NSAT_OK;
+    // table: narrow jobs, then wide ones
+    uint32_t i = 0;
+    for (int c = 0; c < 2; c++)
+        for (size_t q = 0; q < sel[c].size(); q++) {
+            b.h_jobs[i++] = recs[c][q];
+            b.jobs.push_back(sel[c][q]);
+        }
+    b.h_hdr->njobs = k;
+    b.h_hdr->n_narrow = (uint32_t)sel[0].size();
+    if (sel[0].empty()) narrow = 16;    // only wide jobs: the narrow launch finds nothing
+    cudaGraphExec_t& ge = b.graphs[{narrow, wide}];
+    if (!ge) {
+        if (int rc = capture_graph(s, b, narrow, wide, &ge)) {
+            b.graphs.erase({narrow, wide});
+            return rc;
+        }
     }
-    // epoch time: events around the graph replay (table copies included)
-    SCK(cudaEventRecord(s->ev0, ctx_stream(s->ctx)));
-    SCK(cudaGraphLaunch(s->graph, ctx_stream(s->ctx)));
-    SCK(cudaEventRecord(s->ev1, ctx_stream(s->ctx)));
-    SCK(cudaStreamSynchronize(ctx_stream(s->ctx)));
+    cudaStream_t st = ctx_stream(s->ctx);
+    SCK(cudaEventRecord(b.ev0, st));
+    SCK(cudaGraphLaunch(ge, st));
+    SCK(cudaEventRecord(b.ev1, st));
+    b.launched = true;
+    s->launches += wide ? 2 : 1;
+    return NSAT_OK;
+}
+
+// Waits for buffer b's epoch and folds its results into the jobs, in tile
+// order (epochs are processed in launch order).
+int process_epoch(nsat_server* s, EpochBuf& b) {
+    SCK(cudaEventSynchronize(b.ev1));
     float ms = 0;
-    SCK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    SCK(cudaEventElapsedTime(&ms, b.ev0, b.ev1));
     s->device_ms += ms;
     s->epochs++;
-    // results
-    for (uint32_t i = 0; i < k; i++) {
-        Job* j = in_epoch[i];
-        const SrvJob& r = s->h_jobs[i];
+    b.launched = false;
+    for (size_t i = 0; i < b.jobs.size(); i++) {
+        Job* j = b.jobs[i];
+        const SrvJob& r = b.h_jobs[i];
+        j->inflight--;
+        if (j->finished) continue;   // answered by an earlier epoch; this slice ran ahead
         const uint64_t got = r.tile_end - r.tile_begin;
         j->res.tiles += got;
+        j->cursor = r.tile_end;
         bool finished = false;
         if (j->kind == SRV_SAT) {
             j->count += r.count;
             if (r.min_idx != ~0ull && !j->res.satisfiable) {
-                // the first slice with a solution holds the lowest one
+                // every lower tile was in this or an earlier processed epoch
                 j->res.satisfiable = 1;
                 j->res.witness_lo = r.min_idx >> j->d;
                 if (!j->find_all) finished = true;
             }
-            j->cursor = r.tile_end;
             if (j->cursor == j->total_tiles) finished = true;
             j->res.count = j->count >> j->d;
         } else if (j->kind == SRV_QSAT) {
-            j->cursor = r.tile_end;
             j->res.reversed = j->quants[0];
             j->res.solution_bits = j->f;
             if (!j->qr) {
@@ -596,7 +659,7 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
                 }
             } else {
                 for (uint64_t t = 0; t < got && !finished; t++) {
-                    j->qr->push(s->h_vals[r.val_off + t] != 0);
+                    j->qr->push(b.h_vals[r.val_off + t] != 0);
                     FinalResult fr;
                     if (j->qr->final_result(&fr)) {
                         j->res.has_solution = fr.has_solution;
@@ -608,19 +671,47 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
             if (finished) j->res.value = j->res.has_solution ? (j->quants[0] ? 0 : 1) : (j->quants[0] ? 1 : 0);
         } else {
             j->any_stop |= r.any != 0;
-            j->cursor = r.tile_end;
             if (j->cursor == j->total_tiles) {
                 if (int rc = run_joins(s, j)) return rc;
                 finished = true;
             }
         }
-        j->slice = std::min<uint64_t>(j->slice * 2, s->opts.max_slice_tiles);
         if (finished) j->finished = true;
     }
-    // retire finished jobs
+    b.jobs.clear();
+    return NSAT_OK;
+}
+
+}  // namespace
+
+extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_queued) {
+    if (!s) return NSAT_EINVAL;
+    SCK(cudaSetDevice(ctx_device(s->ctx)));
+    // admission in arrival order, by device memory
+    while (!s->queue.empty() && s->active.size() < s->opts.max_active) {
+        Job* j = s->queue.front().get();
+        int a = admit(s, j);
+        if (a < 0) return a;
+        if (a > 0) break;   // does not fit yet
+        s->active.push_back(std::move(s->queue.front()));
+        s->queue.pop_front();
+    }
+    // launch the next epoch, then read the previous one while it runs
+    EpochBuf& next = s->buf[s->cur];
+    EpochBuf& prev = s->buf[s->cur ^ 1];
+    if (int rc = launch_epoch(s, next)) return rc;
+    if (prev.launched) {
+        if (int rc = process_epoch(s, prev)) return rc;
+    } else if (next.launched) {
+        // nothing was in flight: wait for this epoch now (an idle server answers in one step)
+        if (int rc = process_epoch(s, next)) return rc;
+        s->cur ^= 1;
+    }
+    s->cur ^= 1;
+    // retire finished jobs that no launched epoch still reads
     std::vector<std::unique_ptr<Job>> keep;
     for (auto& jp : s->active) {
-        if (jp->finished) {
+        if (jp->finished && jp->inflight == 0) {
             release(s, jp.get());
             finish(s, jp.get());
         } else {
@@ -650,8 +741,9 @@ extern "C" int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st) {
     st->queued = (uint32_t)s->queue.size();
     st->arena_used = s->arena.used;
     st->arena_bytes = s->arena.cap;
-    st->graph_slots = s->graph_slots;
-    st->grid = (uint32_t)s->grid;
+    st->graph_slots = std::max(s->buf[0].max_slots, s->buf[1].max_slots);
+    st->grid = (uint32_t)std::max(s->buf[0].grid, s->buf[1].grid);
+    st->launches = s->launches;
     return NSAT_OK;
 }
 

@@ -36,10 +36,14 @@ static_assert(sizeof(SrvIns) == 16, "SrvIns layout");
 enum { SRV_SAT = 0, SRV_QSAT = 1, SRV_TABLE = 2 };
 
 // Epoch header read by the kernel (so one captured graph serves every epoch).
+// Jobs [0, n_narrow) run in the launch sized for SRV_NARROW_SLOTS slots per
+// warp, jobs [n_narrow, njobs) in the launch sized for the epoch's widest.
 struct SrvEpoch {
     uint32_t njobs;
-    uint32_t pad[63];
+    uint32_t n_narrow;
+    uint32_t pad[62];
 };
+#define SRV_NARROW_SLOTS 48
 
 // Device job record; 256 bytes.  Static fields are written at admission,
 // the slice fields every epoch, the result fields by the kernels.

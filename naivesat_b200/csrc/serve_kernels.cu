@@ -305,10 +305,13 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
 }
 
 // One warp per CTA; the dynamic shared memory is max_slots * SRV_SLOT_BYTES.
+// cls 0 serves the epoch's narrow jobs, cls 1 its wide ones.
 __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict__ hdr, SrvJob* __restrict__ jobs,
-                                                  uint8_t* __restrict__ vals) {
+                                                  uint8_t* __restrict__ vals, u32 cls) {
     extern __shared__ __align__(16) char smem[];
-    const u32 njobs = hdr->njobs;
+    const u32 n_narrow = hdr->n_narrow;
+    const u32 njobs = cls == 0 ? n_narrow : hdr->njobs - n_narrow;
+    if (cls != 0) jobs += n_narrow;
     const u32 lane = threadIdx.x & 31u;
     char* Sl = smem + lane * (W * 4);
     u32 j = njobs ? blockIdx.x % njobs : 0;
@@ -331,17 +334,20 @@ __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict_
 }  // namespace
 
 extern "C" int nsat_launch_serve_epoch(const SrvEpoch* hdr, SrvJob* jobs, uint32_t max_slots, uint8_t* vals,
-                                       int grid, cudaStream_t stream) {
+                                       int grid, uint32_t cls, cudaStream_t stream) {
     // the dynamic shared memory limit was raised by nsat_serve_occupancy
     const size_t smem = (size_t)max_slots * SRV_SLOT_BYTES;
-    serve_epoch<<<grid, 32, smem, stream>>>(hdr, jobs, vals);
+    serve_epoch<<<grid, 32, smem, stream>>>(hdr, jobs, vals, cls);
     return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 
 extern "C" int nsat_serve_occupancy(uint32_t max_slots, int* ctas_per_sm) {
+    if (max_slots > SRV_MAX_SLOTS) return -1;
     const size_t smem = (size_t)max_slots * SRV_SLOT_BYTES;
     const void* fn = (const void*)serve_epoch;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    // the limit covers every slot count, so launches captured earlier stay valid
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_MAX_SLOTS * SRV_SLOT_BYTES) !=
+        cudaSuccess)
         return -4;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32, smem) == cudaSuccess ? 0 : -4;
 }

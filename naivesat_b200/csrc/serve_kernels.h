@@ -6,9 +6,10 @@
 #include "serve_common.h"
 
 extern "C" {
-// grid one-warp CTAs, each with max_slots * SRV_SLOT_BYTES of shared memory
+// grid one-warp CTAs, each with max_slots * SRV_SLOT_BYTES of shared memory,
+// serving the epoch's narrow (cls 0) or wide (cls 1) jobs
 int nsat_launch_serve_epoch(const SrvEpoch* hdr, SrvJob* jobs, uint32_t max_slots, uint8_t* vals, int grid,
-                            cudaStream_t stream);
+                            uint32_t cls, cudaStream_t stream);
 // raises the kernel's shared-memory limit for max_slots and reports CTAs per SM
 int nsat_serve_occupancy(uint32_t max_slots, int* ctas_per_sm);
 }
