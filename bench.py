@@ -2,7 +2,7 @@
 """Benchmark of the naivesat hot path on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload c1|c0|c1_twin|c2a|c2b|c2c|c3a|c3b|c3m|c3s]
+                  [--workload c1|c0|c1_twin|c2a|c2b|c2c|c3a|c3b|c3m|c3s|c4]
 
 Default workload (c1): exhaustive bit-sliced SAT of the 36-input / 3018-gate
 planted random-DAG circuit (seed 1), exact solution count plus lowest witness
@@ -15,7 +15,10 @@ max over ranks.  `--impl reference` times the oracle port of the reference's
 gatenative CPU path on this host's cores instead (rank 0 only).
 
 The other workloads print the same line shape for the QSAT (c2*) and
-SATOSTOP (c3*) paths; their steps are replicas on every rank.
+SATOSTOP (c3*) paths; their steps are replicas on every rank.  c4 is the
+serving trace (10,000 requests): `value` is solves/s with every request
+queued at t=0, `latency` the p50/p99 under Poisson arrivals, `plain` the
+one-launch-per-instance form on the same trace.
 """
 import argparse
 import json
@@ -455,6 +458,162 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------
+# config 4: batched serving
+
+def serving_cpu_baseline(reqs, threads, target_s):
+    """The oracle port solving requests in order on the host cores for about
+    target_s seconds; returns (solves/s, sample description)."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    k = 0
+    for r in reqs:
+        if time.perf_counter() - t0 > target_s:
+            break
+        c = r["circ"]
+        oc = O.Circuit(c.n, c.gates, c.outputs)
+        if r["kind"] == "sat":
+            # growing chunks, ending at the first chunk with a solution (the
+            # lowest witness, as the server reports it)
+            b, span = 0, 1 << min(c.n, 20)
+            while b < (1 << c.n):
+                e = min(1 << c.n, b + span)
+                if O.sat_range(oc, b, e, threads)[1] is not None:
+                    break
+                b, span = e, span * 2
+        elif r["kind"] == "qsat":
+            O.qsat(oc, r["quants"], mode=1, threads=threads)
+        else:
+            O.stop_solve(c.n, r["unknowns"], O.stop_table(oc, threads), mode=1, threads=threads)
+        k += 1
+    dt = time.perf_counter() - t0
+    return k / dt, "first %d requests of the trace in %.1f s" % (k, dt)
+
+
+def run_serving_reference(args, world, rank):
+    """Reference arm of config 4: the oracle port of the reference's CPU path
+    solving the trace's requests one after another on all host cores (the
+    reference runs one circuit per process and has no server)."""
+    if rank != 0:
+        return
+    from naivesat_b200 import workloads as W
+    reqs = W.serving_requests(args.requests, seed=2024, rate_hz=args.rate)
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(max(1, args.steps)):
+        v, sample = serving_cpu_baseline(reqs, threads, 20.0)
+        vals.append(v)
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": 0, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 bit-sliced", "data": "synthetic",
+            "config": {"workload": "config 4 trace, requests solved in order on the host", "cpu": cpu_model()},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args, world, rank, local):
+    """Config 4: 10,000 SAT/QSAT/SATOSTOP requests (70/20/10) with Poisson
+    arrivals through the batched server, against the plain one-launch-per-
+    instance form on the same trace."""
+    if rank != 0:
+        return        # one server per GPU; the trace is served on rank 0's GPU
+    from naivesat_b200 import api, serving, workloads as W
+    ctx = api.Context(local)
+    reqs = W.serving_requests(args.requests, seed=2024, rate_hz=args.rate)
+    warm = W.serving_requests(64, seed=99, rate_hz=1e9)
+    srv_kw = dict(epoch_budget=48000000)
+
+    peak_lop3, probe_mhz = ctx.lop3_peak()
+    srv = api.Server(ctx, **srv_kw)
+    serving.replay_server(srv, warm, realtime=False)      # graphs captured, context warm
+    srv.close()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    srv = api.Server(ctx, **srv_kw)
+    res_sat, lat_sat, mk_sat = serving.replay_server(srv, reqs, realtime=False)
+    st_sat = srv.stats()
+    srv.close()
+    clk = clocks.stop()
+    srv = api.Server(ctx, **srv_kw)
+    res_poi, lat_poi, mk_poi = serving.replay_server(srv, reqs, realtime=True)
+    st_poi = srv.stats()
+    srv.close()
+    for i in res_sat:
+        assert serving.verdict(reqs[i]["kind"], res_sat[i]) == serving.verdict(reqs[i]["kind"], res_poi[i]), i
+
+    # the plain form: one request at a time through the one-shot solvers
+    pres, service = serving.plain_service_times(ctx, reqs, args.plain_seconds)
+    kp = len(service)
+    same = sum(serving.verdict(reqs[i]["kind"], pres[i]) == serving.verdict(reqs[i]["kind"], res_sat[i])
+               for i in pres)
+    assert same == kp, (same, kp)
+    plain_lat = serving.fifo_latencies([r["arrival_s"] for r in reqs[:kp]], service)
+
+    # a rate the plain form sustains: both forms on the same arrivals
+    low = W.serving_requests(max(8, int(args.low_rate * args.low_seconds)), seed=77, rate_hz=args.low_rate)
+    srv = api.Server(ctx, **srv_kw)
+    res_low, lat_low, mk_low = serving.replay_server(srv, low, realtime=True)
+    srv.close()
+    pres_low, svc_low = serving.plain_service_times(ctx, low, 1e9)
+    assert all(serving.verdict(low[i]["kind"], pres_low[i]) == serving.verdict(low[i]["kind"], res_low[i])
+               for i in pres_low)
+    plain_low_lat = serving.fifo_latencies([r["arrival_s"] for r in low], svc_low)
+
+    # interpreter work: tiles x program length (NOPs included) x 1024 words per tile
+    ins = [sum(api.server_program_check(r["circ"], r["kind"])[1:]) for r in reqs]
+    words = sum(res_sat[i]["tiles"] * 1024 * ins[i] for i in res_sat)
+    lut_words = words / (st_sat["device_ms"] * 1e-3)
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, sample = serving_cpu_baseline(reqs, threads, 15.0)
+        cpu = {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample + ", " + cpu_model()}
+    kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("sat", "qsat", "stop")}
+    sat_sum = serving.summarize(lat_sat, mk_sat, len(res_sat))
+    poi_sum = serving.summarize(lat_poi, mk_poi, len(res_poi))
+    line = {
+        "metric": "solves/s", "value": sat_sum["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "steps": len(reqs), "warmup": len(warm), "ms_per_step": 1e3 / sat_sum["solves_per_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 bit-sliced (lop3.b32 LUT interpreter)", "data": "synthetic",
+        "config": {"workload": "config 4: %d requests (%d SAT, %d QSAT, %d SATOSTOP), 18-34 inputs, 100-4000 "
+                               "gates (log-uniform), SATOSTOP <= 20 state bits; server with all requests queued "
+                               "at t=0 (value) and with Poisson arrivals at %.0f/s (latency)"
+                               % (len(reqs), kinds["sat"], kinds["qsat"], kinds["stop"], args.rate),
+                   "step": "one request solved", "epochs": st_sat["epochs"],
+                   "l2": "no memory inputs (assignments come from thread indices)"},
+        "latency": dict(poi_sum, rate_hz=args.rate, epochs=st_poi["epochs"]),
+        "plain": {"form": "one request at a time through the one-shot solvers (per-circuit NVRTC kernel, "
+                          "empty kernel cache, own launches)",
+                  "requests": kp, "solves_per_s": kp / sum(service),
+                  "p50_ms_at_rate": serving.percentile(plain_lat, 50) * 1e3,
+                  "p99_ms_at_rate": serving.percentile(plain_lat, 99) * 1e3,
+                  "latency_note": "FIFO latencies from the measured service times under the same arrivals; "
+                                  "the queue grows without bound at this rate",
+                  "verdicts_equal": same},
+        "low_rate": {"rate_hz": args.low_rate, "requests": len(low),
+                     "server": serving.summarize(lat_low, mk_low, len(res_low)),
+                     "plain": serving.summarize(plain_low_lat, sum(svc_low), len(svc_low))},
+        "roofline": {"bound": "alu", "kernel": "serve_epoch",
+                     "achieved": 7 * lut_words, "peak": peak_lop3, "unit": "lop3/s",
+                     "frac": 7 * lut_words / peak_lop3, "traffic": None,
+                     "lut_words_per_s": lut_words,
+                     "note": "a run-time LUT costs 7 lop3 (mux tree over truth-table masks) per 32-bit word",
+                     "peak_source": "measured lop3.b32 chain microbenchmark on this GPU (%.0f MHz)" % probe_mhz},
+        "cpu_baseline": cpu,
+        "e2e": {"value": sat_sum["solves_per_s"], "unit": "solves/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "the server runs end to end: circuits arrive as host arrays, programs and epoch tables "
+                        "are copied in, results copied out"},
+        "gpu_launches": st_sat["launches"],
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -465,10 +624,20 @@ def main():
     ap.add_argument("--log2", type=int, default=36,
                     help="SAT workloads: enumerate only the first 2^LOG2 assignments (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--requests", type=int, default=10000, help="c4: requests in the trace")
+    ap.add_argument("--rate", type=float, default=150.0, help="c4: Poisson arrival rate (1/s)")
+    ap.add_argument("--plain-seconds", type=float, default=60.0, help="c4: time given to the plain form")
+    ap.add_argument("--low-rate", type=float, default=2.0, help="c4: a rate the plain form sustains")
+    ap.add_argument("--low-seconds", type=float, default=45.0, help="c4: length of the low-rate trace")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.workload == "c4":
+            if args.impl == "reference":
+                run_serving_reference(args, world, rank)
+            else:
+                run_serving(args, world, rank, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_ours(args, world, rank, local)

@@ -48,10 +48,11 @@ def summarize(lat_s, makespan_s, count):
             "mean_ms": sum(lat_s) / len(lat_s) * 1e3 if lat_s else None}
 
 
-def replay_server(srv, reqs, realtime=True, time_limit_s=None):
-    """Submits each request at its arrival time (all at once when realtime is
-    False), steps the server, and collects results.  Returns (results by
-    index, latencies in s, makespan in s)."""
+def replay_server(srv, reqs, realtime=True, time_limit_s=None, burst=128):
+    """Submits each request at its arrival time (all at time 0 when realtime
+    is False), at most `burst` per step so the device starts while a backlog
+    is still being submitted, steps the server, and collects results.
+    Returns (results by index, latencies in s, makespan in s)."""
     t0 = time.perf_counter()
     arrival = [r["arrival_s"] if realtime else 0.0 for r in reqs]
     results, lat = {}, {}
@@ -61,7 +62,9 @@ def replay_server(srv, reqs, realtime=True, time_limit_s=None):
         now = time.perf_counter() - t0
         if time_limit_s is not None and now > time_limit_s:
             break
-        while i < len(reqs) and arrival[i] <= now:
+        b = 0
+        while i < len(reqs) and arrival[i] <= now and b < burst:
+            b += 1
             r = reqs[i]
             srv.submit(r["kind"], r["circ"], quants=r["quants"], unknowns=r["unknowns"], tag=i,
                        find_all=r.get("find_all", False))
@@ -125,6 +128,45 @@ def replay_plain(ctx, reqs, realtime=True, time_limit_s=None, fresh_jit_cache=Tr
             busy += e - s
             lat[i] = (e - t0) - arr
         return results, [lat[k] for k in sorted(lat)], busy
+    finally:
+        if tmp is not None:
+            if old is None:
+                os.environ.pop("NSAT_JIT_CACHE", None)
+            else:
+                os.environ["NSAT_JIT_CACHE"] = old
+            tmp.cleanup()
+
+
+def fifo_latencies(arrivals, service):
+    """Latencies of a single FIFO server with the given service times (the
+    plain form handles one request at a time, so its queueing follows from
+    its measured service times)."""
+    end = 0.0
+    lat = []
+    for a, sv in zip(arrivals, service):
+        start = max(a, end)
+        end = start + sv
+        lat.append(end - a)
+    return lat
+
+
+def plain_service_times(ctx, reqs, time_limit_s, fresh_jit_cache=True):
+    """Solves requests one at a time (back to back) until time_limit_s;
+    returns (results by index, service time of each in s)."""
+    old = os.environ.get("NSAT_JIT_CACHE")
+    tmp = tempfile.TemporaryDirectory(prefix="nsat_plain_") if fresh_jit_cache else None
+    if tmp is not None:
+        os.environ["NSAT_JIT_CACHE"] = tmp.name
+    try:
+        t0 = time.perf_counter()
+        results, service = {}, []
+        for i, req in enumerate(reqs):
+            if time.perf_counter() - t0 > time_limit_s:
+                break
+            s = time.perf_counter()
+            results[i] = solve_one(ctx, req)
+            service.append(time.perf_counter() - s)
+        return results, service
     finally:
         if tmp is not None:
             if old is None:

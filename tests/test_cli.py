@@ -93,6 +93,10 @@ def test_satostop_clis(tmp_path):
     out = run("naivesatostop", path, 16, "-t", "opencl:0", "-v", check=True).stdout
     assert "Solution: Solution { start: 0, end: 0, steps: 16777216 }\n" in out
     assert "Verified: end=0 steps=16777216\n" in out and "INCORRECT" not in out
+    # hashmap tuning flags of the reference's engine are accepted and change nothing
+    out = run("naivesatostop", path, 16, "-t", "cpu", "-H", "20", "-U", "4", "-P", "2", "-C", "10",
+              check=True).stdout
+    assert "Solution: Solution { start: 0, end: 0, steps: 16777216 }\n" in out
     out = run("naivesatostop", path, 16, "-S", check=True).stdout
     assert "Stopped at %s %s\n" % ("0" * 16, "0" * 24) in out
     out = run("greedysatostop", write(tmp_path, W.config("c3a"), "lfsr"), 16, check=True).stdout
