@@ -213,6 +213,37 @@ typedef struct {
 int nsat_stop_solve(nsat_ctx* ctx, nsat_table* t, const nsat_stop_opts* opts,
                     nsat_stop_result* res);
 
+/* ---- partitioned greedysatostop (greedysatostop -p P [-x PREFIX]) -------
+ * Replaces do_solve_with_cpu_builder_with_partitions
+ * (greedysatostop.rs:692-837): the table is kept as a packed image of
+ * (n+1)-bit entries (MemImage/FileImage layout, greedysatostop.rs:308-594)
+ * outside device memory, and joined partition by partition in the
+ * reference's order, so the answer is the reference's for every P.  The
+ * image lives in pinned host memory, or with file_prefix in the temp file
+ * <file_prefix>greedy_temp_<ns> (deleted before return).  Device memory: two
+ * unpacked partitions (2^(n - log2 P) x 8 bytes each) plus one packed one. */
+typedef struct {
+    uint32_t unknowns;
+    uint32_t partitions;        /* power of two >= 2, partitions * 64 <= 2^n */
+    const char* file_prefix;    /* NULL: pinned host memory */
+} nsat_greedy_opts;
+
+typedef struct {
+    int32_t found;
+    uint32_t stage, partition;  /* where the answer was found */
+    uint32_t load_bits;         /* first-pass chunks: 2^load_bits ("Load partition bits") */
+    uint64_t start, end;
+    uint64_t joins;             /* partition joins run */
+    double build_ms, join_ms, wall_ms;   /* table kernels, join kernels (CUDA events); wall */
+    uint64_t h2d_bytes, d2h_bytes;       /* image traffic over PCIe */
+} nsat_greedy_result;
+
+int nsat_greedy_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_greedy_opts* opts, nsat_greedy_result* res);
+/* The packed image after the first pass (ceil(2^n (n+1) / 64) words), for
+ * checking the layout; the partition count sets the first pass's chunking. */
+int nsat_greedy_image(nsat_ctx* ctx, nsat_circuit* c, uint32_t partitions, const char* file_prefix,
+                      uint64_t* words, uint64_t nwords);
+
 /* ---- batched serving ---------------------------------------------------- */
 /* A server runs many SAT / QSAT / SATOSTOP jobs on one device concurrently
  * (no counterpart in the reference, which solves one circuit per process).

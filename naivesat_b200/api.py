@@ -77,6 +77,17 @@ class StopResult(C.Structure):
                 ("join_ms", C.c_double)]
 
 
+class GreedyOpts(C.Structure):
+    _fields_ = [("unknowns", C.c_uint32), ("partitions", C.c_uint32), ("file_prefix", C.c_char_p)]
+
+
+class GreedyResult(C.Structure):
+    _fields_ = [("found", C.c_int32), ("stage", C.c_uint32), ("partition", C.c_uint32),
+                ("load_bits", C.c_uint32), ("start", C.c_uint64), ("end", C.c_uint64),
+                ("joins", C.c_uint64), ("build_ms", C.c_double), ("join_ms", C.c_double),
+                ("wall_ms", C.c_double), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("arena_bytes", C.c_uint64), ("max_active", C.c_uint32), ("max_queue", C.c_uint32),
                 ("max_slice_tiles", C.c_uint32), ("first_slice_tiles", C.c_uint32),
@@ -113,7 +124,7 @@ EXPORTS = [
     "nsat_table_bytes", "nsat_stop_solve", "nsat_probe_lop3_peak", "nsat_jit_check",
     "nsat_qsat_solve_noalloc", "nsat_server_create", "nsat_server_destroy", "nsat_server_submit",
     "nsat_server_step", "nsat_server_poll", "nsat_server_stats", "nsat_gen_random_dag",
-    "nsat_gen_lfsr_stop", "nsat_server_program_check",
+    "nsat_gen_lfsr_stop", "nsat_server_program_check", "nsat_greedy_solve", "nsat_greedy_image",
 ]
 
 _lib = None
@@ -160,6 +171,8 @@ def lib():
         L.nsat_table_bytes.restype = C.c_uint64
         L.nsat_stop_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(StopOpts), C.POINTER(StopResult)]
         L.nsat_probe_lop3_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.nsat_greedy_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(GreedyOpts), C.POINTER(GreedyResult)]
+        L.nsat_greedy_image.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_char_p, U64P, C.c_uint64]
         L.nsat_server_create.argtypes = [C.c_void_p, C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]
         L.nsat_server_destroy.argtypes = [C.c_void_p]
         L.nsat_server_destroy.restype = None
@@ -321,6 +334,28 @@ class CircuitHandle:
 
     def stop_table(self, want_steps=False):
         return Table(self, want_steps)
+
+    def greedy_partitioned(self, unknowns, partitions, file_prefix=None):
+        """greedysatostop -p: the table as a packed image outside device
+        memory (pinned host memory, or a temp file under file_prefix),
+        joined partition by partition in the reference's order."""
+        o = GreedyOpts(unknowns, partitions, file_prefix.encode() if file_prefix is not None else None)
+        r = GreedyResult()
+        self.ctx._check(lib().nsat_greedy_solve(self.ctx.h, self.h, C.byref(o), C.byref(r)), "greedy_solve")
+        d = {f: getattr(r, f) for f, _ in GreedyResult._fields_}
+        d["found"] = bool(r.found)
+        if not r.found:
+            d["start"] = d["end"] = None
+        return d
+
+    def greedy_image(self, partitions, file_prefix=None):
+        """The packed (n+1)-bit table image after the first pass."""
+        words = ((1 << self.n) * (self.n + 1) + 63) // 64
+        out = np.zeros(words, dtype=np.uint64)
+        self.ctx._check(lib().nsat_greedy_image(self.ctx.h, self.h, partitions,
+                                                file_prefix.encode() if file_prefix is not None else None,
+                                                out.ctypes.data_as(U64P), words), "greedy_image")
+        return out
 
 
 KINDS = {"sat": 0, "qsat": 1, "stop": 2}

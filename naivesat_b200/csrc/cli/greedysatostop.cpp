@@ -8,7 +8,11 @@
 // with -v the path is replayed: "Verified: end=E" and "INCORRECT" on a
 // mismatch.  The table lives in device memory (two ping-pong buffers); the
 // start reported is the lowest one among those resolved in the first
-// doubling round that resolves any.
+// doubling round that resolves any.  With -p P the table is a packed image
+// outside device memory (pinned host memory, or with -x PREFIX the temp file
+// PREFIXgreedy_temp_<ns>) joined partition by partition in the reference's
+// order (greedysatostop.rs:692-837), so the answer is the reference's for
+// that P.
 #include "cli_common.h"
 
 using namespace cli;
@@ -34,11 +38,15 @@ int main(int argc, char** argv) {
     if (L.d.output_num != n + 1) die("circuit must have input_len + 1 outputs", 1);
     if (unknowns > n) die("unknowns must not exceed input_len", 1);
     if (n >= 64) die("input_len must be below 64", 1);
+    uint64_t parts = 0;
     if (a.has("partitions")) {
-        uint64_t p = a.num("partitions", 0);
-        if (p < 2) die("Too small number of partitions", 1);
-        if (p & (p - 1)) die("Number of partitions must be power of 2", 1);
-        printf("Partitions: %llu (the table is held in device memory)\n", (unsigned long long)p);
+        parts = a.num("partitions", 0);
+        if (a.has("opencl")) die("partitions run without -C (the reference asserts this)", 101);
+        if (parts < 2) die("Too small number of partitions", 101);
+        if (parts & (parts - 1)) die("Number of partitions must be power of 2", 101);
+        uint32_t pb = 0;
+        while ((1ull << pb) < parts) pb++;
+        printf("Load partition bits: %u\n", std::min<uint32_t>(pb + 2, n - 10));
     }
     const int dev = (int)a.num("opencl", 0);
     nsat_ctx* ctx = open_ctx(dev, a);
@@ -47,14 +55,28 @@ int main(int argc, char** argv) {
     const double t0 = now_s();
     printf("Calculate first nexts\n");
     nsat_table* t = nullptr;
-    nsat_table_opts to{};
-    check(ctx, nsat_stop_table_build(ctx, c, &to, &t), "table build");
-    nsat_stop_opts so{};
-    so.unknowns = (uint32_t)unknowns;
-    so.mode = 0;
     nsat_stop_result r{};
-    check(ctx, nsat_stop_solve(ctx, t, &so, &r), "stop solve");
-    printf("Joining nexts: %u stages\n", r.rounds);
+    if (parts) {
+        nsat_greedy_opts go{};
+        go.unknowns = (uint32_t)unknowns;
+        go.partitions = (uint32_t)parts;
+        const std::string prefix = a.has("file-image-prefix") ? a.get("file-image-prefix") : std::string();
+        go.file_prefix = a.has("file-image-prefix") ? prefix.c_str() : nullptr;
+        nsat_greedy_result gr{};
+        check(ctx, nsat_greedy_solve(ctx, c, &go, &gr), "partitioned solve");
+        printf("Joined %llu partition pairs\n", (unsigned long long)gr.joins);
+        r.found = gr.found;
+        r.start = gr.start;
+        r.end = gr.end;
+    } else {
+        nsat_table_opts to{};
+        check(ctx, nsat_stop_table_build(ctx, c, &to, &t), "table build");
+        nsat_stop_opts so{};
+        so.unknowns = (uint32_t)unknowns;
+        so.mode = 0;
+        check(ctx, nsat_stop_solve(ctx, t, &so, &r), "stop solve");
+        printf("Joining nexts: %u stages\n", r.rounds);
+    }
     printf("Time: %.6f\n", now_s() - t0);
     if (r.found) {
         printf("Solution: Solution { start: %llu, end: %llu }\n", (unsigned long long)r.start,
@@ -77,7 +99,7 @@ int main(int argc, char** argv) {
     } else {
         printf("Unsatisfiable!\n");
     }
-    nsat_table_free(t);
+    if (t) nsat_table_free(t);
     nsat_circuit_free(c);
     nsat_destroy(ctx);
     return 0;

@@ -304,12 +304,13 @@ __device__ __forceinline__ void transpose32(u32* a) {
 }
 
 extern "C" __global__ void NSAT_BOUNDS
-nsat_table(u64 nwords, void* __restrict__ table, LaunchOut* __restrict__ out) {
+nsat_table(u64 nwords, u64 w0, void* __restrict__ table, LaunchOut* __restrict__ out) {
+    // entries of words w0 .. w0+nwords-1 (32 states each), stored from table[0]
     const u64 stride = (u64)gridDim.x * NSAT_NT;
     u32 anystop = 0;
     for (u64 w = (u64)blockIdx.x * NSAT_NT + threadIdx.x; w < nwords; w += stride) {
         u32 x[NSAT_NIN];
-        nsat_inputs_word(x, w);
+        nsat_inputs_word(x, w0 + w);
         u32 o[64];
 #pragma unroll
         for (int k = 0; k < 64; k++) o[k] = 0u;

@@ -31,4 +31,12 @@ int qsat_solve_with_scratch(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quant
                             const nsat_qsat_opts* opts, nsat_qsat_result* res,
                             unsigned char* scratch, size_t scratch_bytes);
 
+// Next-state entries (next | STOP << n, u64) of states first_state ..
+// first_state+count-1 (both multiples of 32) into device memory dev_out, on
+// the context's stream (synchronous); any_stop reports a STOP among them.
+int table_chunk_u64(nsat_ctx* ctx, nsat_circuit* c, uint64_t first_state, uint64_t count, uint64_t* dev_out,
+                    uint32_t* any_stop, float* ms);
+
+const Circuit& circuit_of(const nsat_circuit* c);
+
 }  // namespace nsat

@@ -336,16 +336,19 @@ int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint
     return NSAT_OK;
 }
 
-int plan_table(const Circuit& circ, bool steps, KernelConfig* kc, std::string* err) {
+// chunked: the partitioned solver builds u64 entries chunk by chunk, so the
+// device-memory limit on n does not apply.
+int plan_table(const Circuit& circ, bool steps, KernelConfig* kc, std::string* err, bool chunked = false) {
     const uint32_t n = circ.n;
     if (circ.outputs.size() != n + 1) { *err = "SATOSTOP circuit needs n+1 outputs"; return NSAT_EINVAL; }
-    if (n > 36) { *err = "state longer than 36 bits does not fit device memory"; return NSAT_EUNSUPPORTED; }
+    if (!chunked && n > 36) { *err = "state longer than 36 bits does not fit device memory"; return NSAT_EUNSUPPORTED; }
+    if (n > 62) { *err = "state longer than 62 bits"; return NSAT_EUNSUPPORTED; }
     uint32_t fmt;
     if (steps) {
         if (n > 31) { *err = "steps need n <= 31"; return NSAT_EUNSUPPORTED; }
         fmt = 2;
     } else {
-        fmt = n <= 31 ? 0 : 1;
+        fmt = (n <= 31 && !chunked) ? 0 : 1;
     }
     kc->mode = Mode::TABLE;
     kc->nin = n;
@@ -790,7 +793,8 @@ extern "C" int nsat_stop_table_build(nsat_ctx* ctx, nsat_circuit* c, const nsat_
     unsigned grid = (unsigned)std::min<uint64_t>(want, (uint64_t)ctx->sm_count * 16);
     LaunchOut* po = ctx->d_out;
     void* tb = t->buf[0];
-    void* params[] = {&nwords, &tb, &po};
+    uint64_t w0 = 0;
+    void* params[] = {&nwords, &w0, &tb, &po};
     CK(cudaMemcpyAsync(ctx->d_out, ctx->h_init, sizeof(LaunchOut), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaEventRecord(ctx->ev0[0], ctx->stream));
     if (int rc = launch(ctx, fn, grid, threads, params)) return rc;
@@ -805,6 +809,45 @@ extern "C" int nsat_stop_table_build(nsat_ctx* ctx, nsat_circuit* c, const nsat_
     *out = t.release();
     return NSAT_OK;
 }
+
+namespace nsat {
+
+int table_chunk_u64(nsat_ctx* ctx, nsat_circuit* c, uint64_t first_state, uint64_t count, uint64_t* dev_out,
+                    uint32_t* any_stop, float* ms) {
+    if (int rc = set_device(ctx)) return rc;
+    KernelConfig kc;
+    std::string perr;
+    if (int rc = plan_table(c->circ, false, &kc, &perr, true)) return fail(ctx, rc, perr);
+    const uint32_t n = c->circ.n;
+    if (n < 5 || (first_state & 31) || (count & 31) || count == 0)
+        return fail(ctx, NSAT_EINVAL, "table chunks are whole 32-state words");
+    std::vector<uint32_t> which;
+    for (uint32_t j = 0; j <= n; j++) which.push_back(j);
+    const LutNet& net = get_net(c, which);
+    CUfunction fn;
+    std::shared_ptr<JitModule> mod;
+    if (int rc = get_kernel(ctx, kc, net, "nsat_table", &fn, &mod)) return rc;
+    uint64_t nwords = count >> 5, w0 = first_state >> 5;
+    const unsigned threads = kc.threads();
+    const uint64_t want = (nwords + threads - 1) / threads;
+    const unsigned grid = (unsigned)std::min<uint64_t>(want, (uint64_t)ctx->sm_count * 16);
+    LaunchOut* po = ctx->d_out;
+    void* tb = dev_out;
+    void* params[] = {&nwords, &w0, &tb, &po};
+    CK(cudaMemcpyAsync(ctx->d_out, ctx->h_init, sizeof(LaunchOut), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaEventRecord(ctx->ev0[0], ctx->stream));
+    if (int rc = launch(ctx, fn, grid, threads, params)) return rc;
+    CK(cudaEventRecord(ctx->ev1[0], ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_out, ctx->d_out, sizeof(LaunchOut), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ms) CK(cudaEventElapsedTime(ms, ctx->ev0[0], ctx->ev1[0]));
+    if (any_stop) *any_stop = ctx->h_out[0].any != 0;
+    return NSAT_OK;
+}
+
+const Circuit& circuit_of(const nsat_circuit* c) { return c->circ; }
+
+}  // namespace nsat
 
 extern "C" void nsat_table_free(nsat_table* t) { delete t; }
 

@@ -648,3 +648,53 @@ int or_memimage_find_solution(const uint64_t* data, uint32_t state_len,
     }
     return 0;
 }
+
+/* MemImage::join_nexts (greedysatostop.rs:433-481) on packed partitions of
+ * len entries; second covers states [start2, start2 + len). */
+static void or_join_nexts(uint64_t* dest, const uint64_t* second, uint32_t n, uint64_t len, uint64_t start2) {
+    const uint64_t smask = (1ull << n) - 1, stopbit = 1ull << n;
+    for (uint64_t i = 0; i < len; i++) {
+        const uint64_t v = or_memimage_get(dest, n, i);
+        const uint64_t nx = v & smask;
+        if (!(v & stopbit) && nx >= start2 && nx < start2 + len)
+            or_memimage_set(dest, n, i, or_memimage_get(second, n, nx - start2));
+    }
+}
+
+int or_greedy_partitioned(const uint64_t* table, uint32_t n, uint32_t unknowns, uint32_t partitions,
+                          uint64_t* start, uint64_t* end, uint32_t* stage, uint32_t* part) {
+    if (n < 6 || n > 40 || unknowns > n || partitions < 2 || (partitions & (partitions - 1)) ||
+        (uint64_t)partitions * 64 > (1ull << n))
+        return -1;
+    const uint64_t N = 1ull << n, L = N / partitions;
+    const uint64_t pwords = (L * (n + 1)) >> 6;
+    uint64_t* image = (uint64_t*)calloc((N * (n + 1)) >> 6, 8);
+    uint64_t* dest = (uint64_t*)calloc(pwords, 8);
+    uint64_t* second = (uint64_t*)calloc(pwords, 8);
+    if (!image || !dest || !second) { free(image); free(dest); free(second); return -1; }
+    int have_stop = 0;
+    for (uint64_t s = 0; s < N; s++) {
+        or_memimage_set(image, n, s, table[s]);
+        have_stop |= (table[s] >> n) & 1;
+    }
+    int found = 0;
+    for (uint32_t st = 0; have_stop && st < n && !found; st++) {
+        for (uint32_t i = 0; i < partitions && !found; i++) {
+            memcpy(dest, image + i * pwords, pwords * 8);
+            for (uint32_t j = 0; j < partitions; j++) {
+                if (j != i) memcpy(second, image + j * pwords, pwords * 8);
+                else memcpy(second, dest, pwords * 8);
+                or_join_nexts(dest, second, n, L, (uint64_t)j * L);
+            }
+            if (or_memimage_find_solution(dest, n, (uint64_t)i * L, L, unknowns, start, end) == 1) {
+                *stage = st;
+                *part = i;
+                found = 1;
+            } else {
+                memcpy(image + i * pwords, dest, pwords * 8);
+            }
+        }
+    }
+    free(image); free(dest); free(second);
+    return found;
+}

@@ -95,6 +95,16 @@ int or_memimage_find_solution(const uint64_t* data, uint32_t state_len,
                               uint64_t start, uint64_t len, uint32_t unknowns,
                               uint64_t* sol_start, uint64_t* sol_end);
 
+/* Partitioned greedysatostop (greedysatostop.rs:692-837,
+ * do_solve_with_cpu_builder_with_partitions) on a packed MemImage of the
+ * table T[s] = next | STOP << n: for stage 0..n-1 and partition i, dest =
+ * partition i joined with every partition j in order (the image's current
+ * copy, or dest itself for j == i, greedysatostop.rs:796-806), then
+ * find_solution on dest, else dest is written back.  Returns 1 with the
+ * answer and where it was found, 0 if none, -1 on bad arguments. */
+int or_greedy_partitioned(const uint64_t* table, uint32_t n, uint32_t unknowns, uint32_t partitions,
+                          uint64_t* start, uint64_t* end, uint32_t* stage, uint32_t* part);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,9 @@ def lib():
             L.or_memimage_get.argtypes = [U64P, C.c_uint32, C.c_uint64]
             L.or_memimage_get.restype = C.c_uint64
             L.or_memimage_set.argtypes = [U64P, C.c_uint32, C.c_uint64, C.c_uint64]
+            L.or_greedy_partitioned.argtypes = [U64P, C.c_uint32, C.c_uint32, C.c_uint32,
+                                                C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                                C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
             L.or_memimage_find_solution.argtypes = [U64P, C.c_uint32, C.c_uint64, C.c_uint64,
                                                     C.c_uint32, U64P, U64P]
             _lib = L
@@ -185,6 +188,19 @@ def memimage_get(data, state_len, i):
 
 def memimage_set(data, state_len, i, value):
     lib().or_memimage_set(_ptr(data, U64P), state_len, i, value & 0xFFFFFFFFFFFFFFFF)
+
+
+def greedy_partitioned(n, unknowns, table, partitions):
+    """Partitioned greedysatostop on the table (or_greedy_partitioned)."""
+    t = np.ascontiguousarray(table, dtype=np.uint64)
+    st, en = C.c_uint64(), C.c_uint64()
+    stage, part = C.c_uint32(), C.c_uint32()
+    r = lib().or_greedy_partitioned(_ptr(t, U64P), n, unknowns, partitions, C.byref(st), C.byref(en),
+                                    C.byref(stage), C.byref(part))
+    assert r >= 0, r
+    if r == 0:
+        return None
+    return {"start": st.value, "end": en.value, "stage": stage.value, "partition": part.value}
 
 
 def memimage_find_solution(data, state_len, start, length, unknowns):

@@ -101,3 +101,25 @@ def test_satostop_clis(tmp_path):
     assert "Stopped at %s %s\n" % ("0" * 16, "0" * 24) in out
     out = run("greedysatostop", write(tmp_path, W.config("c3a"), "lfsr"), 16, check=True).stdout
     assert "Unsatisfiable!" in out
+
+
+@gpu
+def test_greedy_partitions_cli(tmp_path):
+    """greedysatostop -p P [-x PREFIX]: the reference's partitioned schedule."""
+    c = W.lfsr_stop(5, 16, 48)
+    path = write(tmp_path, c, "lfsr16")
+    oc = O.Circuit(c.n, c.gates, c.outputs)
+    exp = O.greedy_partitioned(16, 8, O.stop_table(oc), 4)
+    spill = tmp_path / "spill"
+    spill.mkdir()
+    for extra in ([], ["-x", str(spill) + "/"]):
+        out = run("greedysatostop", path, 8, "-p", "4", "-v", *extra, check=True).stdout
+        assert "Load partition bits: 4\n" in out
+        if exp is None:
+            assert "Unsatisfiable!" in out
+        else:
+            assert "Solution: Solution { start: %d, end: %d }\n" % (exp["start"], exp["end"]) in out
+            assert "INCORRECT" not in out
+    assert list(spill.iterdir()) == []
+    p = run("greedysatostop", path, 8, "-p", "3")
+    assert p.returncode == 101 and "power of 2" in p.stderr + p.stdout

@@ -116,3 +116,33 @@ def test_sat_oracle_matches_scalar():
         sols = [v for v in range(1 << c.n) if c.eval_bits([(v >> i) & 1 for i in range(c.n)])[0]]
         assert cnt == len(sols)
         assert low == (sols[0] if sols else None)
+
+
+def test_file_image_partitions_kat():
+    """greedysatostop.rs test_file_image (1271): chunks saved in order form
+    the image, partition p holds entries [p L, (p+1) L), and a saved
+    partition replaces exactly those entries.  Same generator (i * mult +
+    add, then (i + changer) * mult + add), at state_len 14 instead of 26 to
+    keep the CPU suite short."""
+    c = load("greedy_file_image.json")[0]
+    sl, mult, add, parts, changer = 14, c["mult"], c["add"], 16, c["changer"]
+    m64 = (1 << 64) - 1
+    mask = (1 << (sl + 1)) - 1
+    n = 1 << sl
+    img = np.zeros((n * (sl + 1)) // 64, dtype=np.uint64)
+    for i in range(n):                         # save_chunk x 2 * parts, in order
+        O.memimage_set(img, sl, i, (i * mult + add) & m64)
+    plen = n // parts
+    pwords = plen * (sl + 1) // 64
+    for p in reversed(range(parts)):           # load_partition
+        part = img[p * pwords:(p + 1) * pwords]
+        for ci in range(0, plen, 37):
+            i = plen * p + ci
+            assert O.memimage_get(part, sl, ci) == ((i * mult + add) & m64) & mask
+    for p in reversed(range(parts)):           # save_partition
+        part = np.zeros(pwords, dtype=np.uint64)
+        for ci in range(plen):
+            O.memimage_set(part, sl, ci, ((plen * p + ci + changer) * mult + add) & m64)
+        img[p * pwords:(p + 1) * pwords] = part
+    for i in range(0, n, 29):
+        assert O.memimage_get(img, sl, i) == ((i + changer) * mult + add) & m64 & mask
