@@ -2,7 +2,7 @@
 """Benchmark of the naivesat hot path on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload c1|c0|c1_twin|c2a|c2b|c2c|c3a|c3b|c3m|c3s|c4]
+                  [--workload c1|c0|c1_twin|c2a|c2b|c2c|c3a|c3b|c3m|c3s|c3p|c3p_spill|c4]
 
 Default workload (c1): exhaustive bit-sliced SAT of the 36-input / 3018-gate
 planted random-DAG circuit (seed 1), exact solution count plus lowest witness
@@ -297,7 +297,69 @@ class StopWorkload:
         return bytes_ / dt / 1e9, "full oracle table + doubling (%.1f s, u64 arrays)" % dt
 
 
+class StopPartWorkload:
+    """Partitioned greedysatostop (-p): packed (n+1)-bit image, partition
+    joins in the reference's order; the image in device memory (c3p) or
+    spilled to pinned host memory (c3p_spill)."""
+    metric = "join GB/s"
+    kind = "stop"
+
+    def __init__(self, name):
+        from naivesat_b200 import workloads as W
+        self.name = name
+        self.n, self.u, self.P = 28, 20, 4
+        self.circ = W.lfsr_stop(4, self.n, 300)
+        self.spill = name.endswith("spill")
+
+    def describe(self):
+        c = self.circ
+        return {"workload": "greedysatostop -p %d %s: %d-bit LFSR state, %d unknowns, %d gates, packed %d-bit "
+                            "image %s" % (self.P, self.name, c.n, self.u, c.num_gates, c.n + 1,
+                                          "in pinned host memory (PCIe per partition)" if self.spill else
+                                          "in device memory"),
+                "state_bits": c.n, "unknowns": self.u, "partitions": self.P, "gates": c.num_gates}
+
+    def setup(self, ctx, world, rank):
+        self.ctx = ctx
+        self.h = ctx.circuit(self.circ)
+
+    def step(self, fresh=False):
+        h = self.ctx.circuit(self.circ) if fresh else self.h
+        r = h.greedy_partitioned(self.u, self.P, device_bytes=1 if self.spill else 0)
+        self.last = r
+        ms = r["build_ms"] + r["join_ms"] if not self.spill else r["wall_ms"]
+        return {"device_ms": ms, "launches": int(r["joins"]) * 2 + (1 << r["load_bits"]) * 2,
+                "sig": (r["found"], r["start"], r["end"], r["stage"], r["partition"]), "result": r}
+
+    def join_bytes(self):
+        # per join launch: every entry of dest is read (8 B); the entries whose
+        # next state lies in the joined partition, 1/P of them for uniformly
+        # spread next states, gather one entry and write dest (8 + 8 B)
+        return self.last["joins"] * (1 << (self.n - 2)) * (8 + 16 / self.P)
+
+    def work(self):
+        return self.join_bytes() / 1e9
+
+    def roofline(self, world, dev_ms_per_step, peak_lop3, probe_mhz):
+        peak, src = measured_hbm_gbs()
+        r = self.last
+        ach = self.join_bytes() / (r["join_ms"] * 1e-3) / 1e9
+        out = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": None,
+               "peak_source": "%s hbm_gbs (MEASURED_PEAKS.json)" % src, "kernel": "join_packed_kernel",
+               "algorithmic_bytes_per_entry_join": 8 + 16 / self.P,
+               "joins": r["joins"], "join_ms": r["join_ms"], "build_ms": r["build_ms"], "wall_ms": r["wall_ms"],
+               "storage": ["device", "pinned host", "file"][r["storage"]]}
+        if self.spill:
+            out["pcie_gbs"] = (r["h2d_bytes"] + r["d2h_bytes"]) / (r["wall_ms"] * 1e-3) / 1e9
+        return out
+
+    def cpu(self, threads, target_s=12.0):
+        return None, "the oracle's partitioned schedule runs on packed entries one at a time; n=28 is out of reach"
+
+
 def make_workload(name, log2):
+    if name in ("c3p", "c3p_spill"):
+        return StopPartWorkload(name)
     if name in ("c0", "c1", "c1_twin"):
         return SatWorkload(name, log2)
     if name in ("c2a", "c2b", "c2c"):

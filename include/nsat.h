@@ -217,21 +217,27 @@ int nsat_stop_solve(nsat_ctx* ctx, nsat_table* t, const nsat_stop_opts* opts,
  * Replaces do_solve_with_cpu_builder_with_partitions
  * (greedysatostop.rs:692-837): the table is kept as a packed image of
  * (n+1)-bit entries (MemImage/FileImage layout, greedysatostop.rs:308-594)
- * outside device memory, and joined partition by partition in the
- * reference's order, so the answer is the reference's for every P.  The
- * image lives in pinned host memory, or with file_prefix in the temp file
- * <file_prefix>greedy_temp_<ns> (deleted before return).  Device memory: two
- * unpacked partitions (2^(n - log2 P) x 8 bytes each) plus one packed one. */
+ * and joined partition by partition in the reference's order, so the answer
+ * is the reference's for every P.  The image lives in device memory when it
+ * fits, else in pinned host memory (partitions cross PCIe, double-buffered),
+ * or with file_prefix in the temp file <file_prefix>greedy_temp_<ns>
+ * (deleted before return).  Work buffers: two unpacked partitions
+ * (2^(n - log2 P) x 8 bytes each), plus staging for a host or file image. */
 typedef struct {
     uint32_t unknowns;
     uint32_t partitions;        /* power of two >= 2, partitions * 64 <= 2^n */
-    const char* file_prefix;    /* NULL: pinned host memory */
+    const char* file_prefix;    /* image in a temp file under this prefix (greedysatostop -x) */
+    uint64_t device_bytes;      /* without a file: the image stays in device memory when it and the
+                                   work buffers fit in this many bytes (0 = free device memory less
+                                   1 GiB), else it spills to pinned host memory */
 } nsat_greedy_opts;
 
 typedef struct {
     int32_t found;
     uint32_t stage, partition;  /* where the answer was found */
     uint32_t load_bits;         /* first-pass chunks: 2^load_bits ("Load partition bits") */
+    uint32_t storage;           /* where the image lived: 0 device memory, 1 pinned host memory, 2 file */
+    uint32_t reserved;
     uint64_t start, end;
     uint64_t joins;             /* partition joins run */
     double build_ms, join_ms, wall_ms;   /* table kernels, join kernels (CUDA events); wall */

@@ -78,12 +78,14 @@ class StopResult(C.Structure):
 
 
 class GreedyOpts(C.Structure):
-    _fields_ = [("unknowns", C.c_uint32), ("partitions", C.c_uint32), ("file_prefix", C.c_char_p)]
+    _fields_ = [("unknowns", C.c_uint32), ("partitions", C.c_uint32), ("file_prefix", C.c_char_p),
+                ("device_bytes", C.c_uint64)]
 
 
 class GreedyResult(C.Structure):
     _fields_ = [("found", C.c_int32), ("stage", C.c_uint32), ("partition", C.c_uint32),
-                ("load_bits", C.c_uint32), ("start", C.c_uint64), ("end", C.c_uint64),
+                ("load_bits", C.c_uint32), ("storage", C.c_uint32), ("reserved", C.c_uint32),
+                ("start", C.c_uint64), ("end", C.c_uint64),
                 ("joins", C.c_uint64), ("build_ms", C.c_double), ("join_ms", C.c_double),
                 ("wall_ms", C.c_double), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
@@ -335,11 +337,13 @@ class CircuitHandle:
     def stop_table(self, want_steps=False):
         return Table(self, want_steps)
 
-    def greedy_partitioned(self, unknowns, partitions, file_prefix=None):
-        """greedysatostop -p: the table as a packed image outside device
-        memory (pinned host memory, or a temp file under file_prefix),
-        joined partition by partition in the reference's order."""
-        o = GreedyOpts(unknowns, partitions, file_prefix.encode() if file_prefix is not None else None)
+    def greedy_partitioned(self, unknowns, partitions, file_prefix=None, device_bytes=0):
+        """greedysatostop -p: the table as a packed image (device memory when
+        it fits in device_bytes, 0 = free memory; else pinned host memory; or
+        a temp file under file_prefix), joined partition by partition in the
+        reference's order.  result["storage"]: 0 device, 1 host, 2 file."""
+        o = GreedyOpts(unknowns, partitions, file_prefix.encode() if file_prefix is not None else None,
+                       device_bytes)
         r = GreedyResult()
         self.ctx._check(lib().nsat_greedy_solve(self.ctx.h, self.h, C.byref(o), C.byref(r)), "greedy_solve")
         d = {f: getattr(r, f) for f, _ in GreedyResult._fields_}

@@ -2,12 +2,14 @@
 // drop-in for do_solve_with_cpu_builder_with_partitions
 // (greedysatostop.rs:692-837) with the table and the joins on the device.
 //
-// The whole next-state table lives in a packed image of (n+1)-bit entries
-// (the reference's MemImage/FileImage layout, greedysatostop.rs:308-594):
-// in pinned host memory, or, with a file prefix, in the temp file
-// PREFIXgreedy_temp_<ns> that is deleted when the solve returns (the
-// reference's FileImage).  The schedule is the reference's, so answers agree
-// for every partition count:
+// The whole next-state table is a packed image of (n+1)-bit entries (the
+// reference's MemImage/FileImage layout, greedysatostop.rs:308-594).  It
+// lives in device memory when it fits next to the work buffers; otherwise in
+// pinned host memory, partitions crossing PCIe on a copy stream that
+// prefetches the next partition while the current join runs; or, with a file
+// prefix, in the temp file PREFIXgreedy_temp_<ns> (the reference's
+// FileImage), deleted when the solve returns.  The schedule is the
+// reference's, so answers agree for every partition count:
 //   first pass: 2^lb chunks (lb = min(log2 P + 2, n - 10)) of entries built
 //   in order; no STOP anywhere -> no solution;
 //   stage 0..n-1, partition i = 0..P-1: dest = partition i; for j = 0..P-1
@@ -15,15 +17,17 @@
 //   this stage), or, for j == i, a copy of dest as it is at that point; then
 //   the lowest unknown start of dest with STOP is the answer, else dest is
 //   written back.
-// Device memory: two unpacked partitions (dest, second), one packed partition
-// and one chunk of the first pass.
+// dest is unpacked to u64 entries for the race-free in-place join; the other
+// partitions are read packed by the join's gathers.
 #include <cuda_runtime.h>
 #include <fcntl.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "greedy_kernels.h"
 #include "internal.h"
@@ -33,26 +37,11 @@ using namespace nsat;
 
 namespace {
 
+enum Storage { DEVICE = 0, HOST = 1, FILEIMG = 2 };
+
 double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
-
-// Where the packed image lives: pinned host memory or a temp file.
-struct Image {
-    uint64_t bytes = 0;
-    uint64_t* host = nullptr;      // pinned, whole image (no file)
-    int fd = -1;
-    std::string path;
-    uint64_t* stage = nullptr;     // pinned staging for the file case (one partition or chunk)
-    uint64_t stage_bytes = 0;
-
-    ~Image() {
-        if (host) cudaFreeHost(host);
-        if (stage) cudaFreeHost(stage);
-        if (fd >= 0) close(fd);
-        if (!path.empty()) unlink(path.c_str());
-    }
-};
 
 bool pread_all(int fd, void* buf, uint64_t len, uint64_t off) {
     char* p = static_cast<char*>(buf);
@@ -74,18 +63,48 @@ bool pwrite_all(int fd, const void* buf, uint64_t len, uint64_t off) {
     return true;
 }
 
-struct DevBufs {
-    uint64_t* dest = nullptr;
-    uint64_t* second = nullptr;
-    uint64_t* packed = nullptr;
-    uint64_t* chunk = nullptr;
+// Packed bytes of `count` entries of `bits` bits (count a multiple of 64).
+uint64_t packed_bytes(uint64_t count, uint32_t bits) { return ((count * bits) >> 6) * 8; }
+
+// The image and every buffer the solve uses.
+struct Work {
+    int storage = DEVICE;
+    uint64_t bytes = 0;
+    uint64_t* dev_image = nullptr;    // DEVICE
+    uint64_t* host_image = nullptr;   // HOST (pinned)
+    int fd = -1;                      // FILEIMG
+    std::string path;
+    uint64_t* host_stage = nullptr;   // FILEIMG: pinned staging of one partition or chunk
+    uint64_t* dest = nullptr;         // unpacked partition i
+    uint64_t* snap = nullptr;         // unpacked copy of dest (j == i)
+    uint64_t* stage[2] = {nullptr, nullptr};   // HOST/FILEIMG: packed partitions on the device
+    uint64_t* chunk = nullptr;        // first pass: u64 entries of one chunk
     uint64_t* best = nullptr;
-    ~DevBufs() {
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ready[2] = {nullptr, nullptr}, used[2] = {nullptr, nullptr};
+    cudaEvent_t wb = nullptr;
+    std::vector<cudaEvent_t> jev;     // a start/end pair per join of one partition step
+
+    ~Work() {
+        if (copy) cudaStreamSynchronize(copy);
+        cudaFree(dev_image);
         cudaFree(dest);
-        cudaFree(second);
-        cudaFree(packed);
+        cudaFree(snap);
+        cudaFree(stage[0]);
+        cudaFree(stage[1]);
         cudaFree(chunk);
         cudaFree(best);
+        if (host_image) cudaFreeHost(host_image);
+        if (host_stage) cudaFreeHost(host_stage);
+        for (int k = 0; k < 2; k++) {
+            if (ready[k]) cudaEventDestroy(ready[k]);
+            if (used[k]) cudaEventDestroy(used[k]);
+        }
+        for (cudaEvent_t e : jev) cudaEventDestroy(e);
+        if (wb) cudaEventDestroy(wb);
+        if (copy) cudaStreamDestroy(copy);
+        if (fd >= 0) close(fd);
+        if (!path.empty()) unlink(path.c_str());
     }
 };
 
@@ -102,84 +121,6 @@ struct DevBufs {
         if ((call) != 0) return ctx_fail(ctx, NSAT_ECUDA, std::string(#call) + " failed");         \
     } while (0)
 
-// Packed bytes of `count` entries of `bits` bits (count a multiple of 64).
-uint64_t packed_bytes(uint64_t count, uint32_t bits) { return ((count * bits) >> 6) * 8; }
-
-// Copies a packed range of the image (byte offset off, len bytes) to the
-// device, through the staging buffer in the file case.
-int image_to_device(nsat_ctx* ctx, Image& im, uint64_t off, uint64_t len, void* dev, cudaStream_t st,
-                    nsat_greedy_result* r) {
-    if (im.host) {
-        GCK(cudaMemcpyAsync(dev, reinterpret_cast<char*>(im.host) + off, len, cudaMemcpyHostToDevice, st));
-    } else {
-        if (!pread_all(im.fd, im.stage, len, off)) return ctx_fail(ctx, NSAT_EINVAL, "image file read failed");
-        GCK(cudaMemcpyAsync(dev, im.stage, len, cudaMemcpyHostToDevice, st));
-        GCK(cudaStreamSynchronize(st));   // the staging buffer is reused next
-    }
-    r->h2d_bytes += len;
-    return NSAT_OK;
-}
-
-int device_to_image(nsat_ctx* ctx, Image& im, uint64_t off, uint64_t len, const void* dev, cudaStream_t st,
-                    nsat_greedy_result* r) {
-    if (im.host) {
-        GCK(cudaMemcpyAsync(reinterpret_cast<char*>(im.host) + off, dev, len, cudaMemcpyDeviceToHost, st));
-    } else {
-        GCK(cudaMemcpyAsync(im.stage, dev, len, cudaMemcpyDeviceToHost, st));
-        GCK(cudaStreamSynchronize(st));
-        if (!pwrite_all(im.fd, im.stage, len, off)) return ctx_fail(ctx, NSAT_EINVAL, "image file write failed");
-    }
-    r->d2h_bytes += len;
-    return NSAT_OK;
-}
-
-// First pass: every chunk of entries, packed, into the image in order.
-int build_image(nsat_ctx* ctx, nsat_circuit* c, Image& im, DevBufs& d, uint32_t lb, bool* any_stop,
-                nsat_greedy_result* r) {
-    const uint32_t n = circuit_of(c).n, bits = n + 1;
-    const uint64_t chunk = 1ull << (n - lb);
-    const uint64_t cbytes = packed_bytes(chunk, bits);
-    cudaStream_t st = ctx_stream(ctx);
-    const int sms = ctx_sm_count(ctx);
-    *any_stop = false;
-    for (uint64_t a = 0; a < (1ull << lb); a++) {
-        uint32_t stop = 0;
-        float ms = 0;
-        if (int rc = table_chunk_u64(ctx, c, a * chunk, chunk, d.chunk, &stop, &ms)) return rc;
-        r->build_ms += ms;
-        *any_stop |= stop != 0;
-        KCK(nsat_greedy_pack(d.chunk, chunk, bits, d.packed, sms, st));
-        if (int rc = device_to_image(ctx, im, a * cbytes, cbytes, d.packed, st, r)) return rc;
-    }
-    return cudaStreamSynchronize(st) == cudaSuccess ? NSAT_OK : ctx_fail(ctx, NSAT_ECUDA, "first pass failed");
-}
-
-int open_image(nsat_ctx* ctx, Image& im, uint64_t bytes, uint64_t stage_bytes, const char* prefix) {
-    im.bytes = bytes;
-    if (!prefix) {
-        cudaError_t e = cudaMallocHost(&im.host, bytes);
-        if (e != cudaSuccess) {
-            im.host = nullptr;
-            return ctx_fail(ctx, NSAT_ENOMEM, "pinned host image of " + std::to_string(bytes) + " bytes: " +
-                                                  cudaGetErrorString(e));
-        }
-        return NSAT_OK;
-    }
-    const long long ns = (long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
-                             std::chrono::system_clock::now().time_since_epoch()).count();
-    im.path = std::string(prefix) + "greedy_temp_" + std::to_string(ns);
-    im.fd = open(im.path.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0600);
-    if (im.fd < 0) {
-        const std::string p = im.path;
-        im.path.clear();
-        return ctx_fail(ctx, NSAT_EINVAL, "cannot create image file " + p);
-    }
-    if (ftruncate(im.fd, (off_t)bytes) != 0) return ctx_fail(ctx, NSAT_ENOMEM, "cannot size image file");
-    GCK(cudaMallocHost(&im.stage, stage_bytes));
-    im.stage_bytes = stage_bytes;
-    return NSAT_OK;
-}
-
 int check_opts(nsat_ctx* ctx, uint32_t n, const nsat_greedy_opts* o, uint32_t* pbits) {
     const uint32_t P = o->partitions;
     if (P < 2 || (P & (P - 1))) return ctx_fail(ctx, NSAT_EINVAL, "partitions must be a power of two >= 2");
@@ -189,6 +130,196 @@ int check_opts(nsat_ctx* ctx, uint32_t n, const nsat_greedy_opts* o, uint32_t* p
     uint32_t b = 0;
     while ((1u << b) < P) b++;
     *pbits = b;
+    return NSAT_OK;
+}
+
+// Chooses where the image lives and allocates the image and work buffers.
+int setup(nsat_ctx* ctx, Work& w, uint32_t n, uint64_t L, uint64_t chunk, const nsat_greedy_opts* o,
+          bool joins) {
+    const uint32_t P = o->partitions;
+    const uint32_t bits = n + 1;
+    w.bytes = packed_bytes(1ull << n, bits);
+    const uint64_t pbytes = packed_bytes(L, bits), cbytes = packed_bytes(chunk, bits);
+    const uint64_t work_dev = (joins ? 2 * L * 8 : 0) + chunk * 8 + 64;
+    if (o->file_prefix) {
+        w.storage = FILEIMG;
+    } else {
+        uint64_t budget = o->device_bytes;
+        if (!budget) {
+            size_t fr = 0, tot = 0;
+            GCK(cudaMemGetInfo(&fr, &tot));
+            budget = fr > (1ull << 30) ? fr - (1ull << 30) : 0;
+        }
+        w.storage = (w.bytes + work_dev <= budget) ? DEVICE : HOST;
+    }
+    if (w.storage == DEVICE) {
+        GCK(cudaMalloc(&w.dev_image, w.bytes));
+    } else {
+        for (int k = 0; k < 2; k++) GCK(cudaMalloc(&w.stage[k], std::max(pbytes, cbytes)));
+        if (w.storage == HOST) {
+            cudaError_t e = cudaMallocHost(&w.host_image, w.bytes);
+            if (e != cudaSuccess) {
+                w.host_image = nullptr;
+                return ctx_fail(ctx, NSAT_ENOMEM, "pinned host image of " + std::to_string(w.bytes) + " bytes: " +
+                                                      cudaGetErrorString(e));
+            }
+        } else {
+            const long long ns = (long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                     std::chrono::system_clock::now().time_since_epoch()).count();
+            w.path = std::string(o->file_prefix) + "greedy_temp_" + std::to_string(ns);
+            w.fd = open(w.path.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0600);
+            if (w.fd < 0) {
+                const std::string p = w.path;
+                w.path.clear();
+                return ctx_fail(ctx, NSAT_EINVAL, "cannot create image file " + p);
+            }
+            if (ftruncate(w.fd, (off_t)w.bytes) != 0) return ctx_fail(ctx, NSAT_ENOMEM, "cannot size image file");
+            GCK(cudaMallocHost(&w.host_stage, std::max(pbytes, cbytes)));
+        }
+    }
+    GCK(cudaMalloc(&w.chunk, chunk * 8));
+    GCK(cudaMalloc(&w.best, 8));
+    if (joins) {
+        GCK(cudaMalloc(&w.dest, L * 8));
+        GCK(cudaMalloc(&w.snap, L * 8));
+    }
+    GCK(cudaStreamCreateWithFlags(&w.copy, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+        GCK(cudaEventCreateWithFlags(&w.ready[k], cudaEventDisableTiming));
+        GCK(cudaEventCreateWithFlags(&w.used[k], cudaEventDisableTiming));
+    }
+    GCK(cudaEventCreateWithFlags(&w.wb, cudaEventDisableTiming));
+    if (joins) {
+        w.jev.assign(2 * P, nullptr);
+        for (auto& e : w.jev) GCK(cudaEventCreate(&e));
+    }
+    return NSAT_OK;
+}
+
+// Packed range of the image at byte offset off -> device buffer dst, on
+// stream st.  HOST: async from pinned memory; FILEIMG: through the pinned
+// staging buffer (synchronous, the staging buffer is reused next).
+int fetch(nsat_ctx* ctx, Work& w, uint64_t off, uint64_t len, void* dst, cudaStream_t st, nsat_greedy_result* r) {
+    if (w.storage == HOST) {
+        GCK(cudaMemcpyAsync(dst, reinterpret_cast<char*>(w.host_image) + off, len, cudaMemcpyHostToDevice, st));
+    } else {
+        if (!pread_all(w.fd, w.host_stage, len, off)) return ctx_fail(ctx, NSAT_EINVAL, "image file read failed");
+        GCK(cudaMemcpyAsync(dst, w.host_stage, len, cudaMemcpyHostToDevice, st));
+        GCK(cudaStreamSynchronize(st));
+    }
+    r->h2d_bytes += len;
+    return NSAT_OK;
+}
+
+int store(nsat_ctx* ctx, Work& w, uint64_t off, uint64_t len, const void* src, cudaStream_t st,
+          nsat_greedy_result* r) {
+    if (w.storage == HOST) {
+        GCK(cudaMemcpyAsync(reinterpret_cast<char*>(w.host_image) + off, src, len, cudaMemcpyDeviceToHost, st));
+    } else {
+        GCK(cudaMemcpyAsync(w.host_stage, src, len, cudaMemcpyDeviceToHost, st));
+        GCK(cudaStreamSynchronize(st));
+        if (!pwrite_all(w.fd, w.host_stage, len, off)) return ctx_fail(ctx, NSAT_EINVAL, "image file write failed");
+    }
+    r->d2h_bytes += len;
+    return NSAT_OK;
+}
+
+// First pass: every chunk of entries, packed, into the image in order.
+int build_image(nsat_ctx* ctx, nsat_circuit* c, Work& w, uint32_t lb, bool* any_stop, nsat_greedy_result* r) {
+    const uint32_t n = circuit_of(c).n, bits = n + 1;
+    const uint64_t chunk = 1ull << (n - lb);
+    const uint64_t cbytes = packed_bytes(chunk, bits);
+    cudaStream_t st = ctx_stream(ctx);
+    const int sms = ctx_sm_count(ctx);
+    *any_stop = false;
+    for (uint64_t a = 0; a < (1ull << lb); a++) {
+        uint32_t stop = 0;
+        float ms = 0;
+        if (int rc = table_chunk_u64(ctx, c, a * chunk, chunk, w.chunk, &stop, &ms)) return rc;
+        r->build_ms += ms;
+        *any_stop |= stop != 0;
+        if (w.storage == DEVICE) {
+            KCK(nsat_greedy_pack(w.chunk, chunk, bits, w.dev_image + a * (cbytes / 8), sms, st));
+        } else {
+            KCK(nsat_greedy_pack(w.chunk, chunk, bits, w.stage[0], sms, st));
+            if (int rc = store(ctx, w, a * cbytes, cbytes, w.stage[0], st, r)) return rc;
+            GCK(cudaStreamSynchronize(st));   // stage[0] is packed into again next
+        }
+    }
+    GCK(cudaStreamSynchronize(st));
+    return NSAT_OK;
+}
+
+// One stage step for partition i: dest = partition i joined with every
+// partition in order.  HOST images prefetch partition j+1 on the copy stream
+// while partition j is joined.
+int join_partition(nsat_ctx* ctx, Work& w, uint32_t n, uint32_t P, uint64_t L, uint32_t i, nsat_greedy_result* r) {
+    const uint32_t bits = n + 1;
+    const uint64_t pbytes = packed_bytes(L, bits), pwords = pbytes / 8;
+    cudaStream_t st = ctx_stream(ctx);
+    const int sms = ctx_sm_count(ctx);
+    // dest
+    if (w.storage == DEVICE) {
+        KCK(nsat_greedy_unpack(w.dev_image + (uint64_t)i * pwords, L, bits, w.dest, sms, st));
+    } else {
+        if (int rc = fetch(ctx, w, (uint64_t)i * pbytes, pbytes, w.stage[0], st, r)) return rc;
+        KCK(nsat_greedy_unpack(w.stage[0], L, bits, w.dest, sms, st));
+    }
+    // the partitions other than i, in order; HOST: double-buffered prefetch
+    std::vector<uint32_t> others;
+    for (uint32_t j = 0; j < P; j++)
+        if (j != i) others.push_back(j);
+    if (w.storage == HOST) {
+        // the copy stream waits for everything issued so far (the write-back
+        // of earlier partitions of this stage and dest's own staging)
+        GCK(cudaEventRecord(w.wb, st));
+        GCK(cudaStreamWaitEvent(w.copy, w.wb, 0));
+        GCK(cudaMemcpyAsync(w.stage[0], reinterpret_cast<char*>(w.host_image) + (uint64_t)others[0] * pbytes, pbytes,
+                            cudaMemcpyHostToDevice, w.copy));
+        GCK(cudaEventRecord(w.ready[0], w.copy));
+        r->h2d_bytes += pbytes;
+    }
+    size_t k = 0;   // next entry of `others`
+    for (uint32_t j = 0; j < P; j++) {
+        const uint64_t* src = nullptr;
+        bool packed = true;
+        int slot = (int)(k & 1);
+        if (j == i) {
+            GCK(cudaMemcpyAsync(w.snap, w.dest, L * 8, cudaMemcpyDeviceToDevice, st));
+            src = w.snap;
+            packed = false;
+        } else if (w.storage == DEVICE) {
+            src = w.dev_image + (uint64_t)j * pwords;
+        } else if (w.storage == HOST) {
+            GCK(cudaStreamWaitEvent(st, w.ready[slot], 0));
+            src = w.stage[slot];
+            if (k + 1 < others.size()) {
+                const int ns = slot ^ 1;
+                if (k >= 1) GCK(cudaStreamWaitEvent(w.copy, w.used[ns], 0));   // its last join is done
+                GCK(cudaMemcpyAsync(w.stage[ns], reinterpret_cast<char*>(w.host_image) + (uint64_t)others[k + 1] * pbytes,
+                                    pbytes, cudaMemcpyHostToDevice, w.copy));
+                GCK(cudaEventRecord(w.ready[ns], w.copy));
+                r->h2d_bytes += pbytes;
+            }
+        } else {
+            if (int rc = fetch(ctx, w, (uint64_t)j * pbytes, pbytes, w.stage[0], st, r)) return rc;
+            src = w.stage[0];
+        }
+        GCK(cudaEventRecord(w.jev[2 * j], st));
+        if (packed) KCK(nsat_greedy_join_packed(w.dest, L, src, (uint64_t)j * L, L, n, sms, st));
+        else KCK(nsat_greedy_join(w.dest, L, src, (uint64_t)j * L, L, n, sms, st));
+        GCK(cudaEventRecord(w.jev[2 * j + 1], st));
+        if (j != i && w.storage == HOST) GCK(cudaEventRecord(w.used[slot], st));
+        if (j != i) k++;
+        r->joins++;
+    }
+    // join kernel time (each pair brackets one launch)
+    GCK(cudaEventSynchronize(w.jev[2 * P - 1]));
+    for (uint32_t j = 0; j < P; j++) {
+        float ms = 0;
+        GCK(cudaEventElapsedTime(&ms, w.jev[2 * j], w.jev[2 * j + 1]));
+        r->join_ms += ms;
+    }
     return NSAT_OK;
 }
 
@@ -208,63 +339,31 @@ extern "C" int nsat_greedy_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_gree
     r->load_bits = lb;
     const uint64_t L = 1ull << (n - pbits);          // entries per partition
     const uint64_t chunk = 1ull << (n - lb);
-    const uint64_t pbytes = packed_bytes(L, bits), cbytes = packed_bytes(chunk, bits);
+    const uint64_t pbytes = packed_bytes(L, bits), pwords = pbytes / 8;
     GCK(cudaSetDevice(ctx_device(ctx)));
-    Image im;
-    if (int rc = open_image(ctx, im, packed_bytes(1ull << n, bits), std::max(pbytes, cbytes), o->file_prefix))
-        return rc;
-    DevBufs d;
-    GCK(cudaMalloc(&d.chunk, chunk * 8));
-    GCK(cudaMalloc(&d.packed, std::max(pbytes, cbytes)));
+    Work w;
+    if (int rc = setup(ctx, w, n, L, chunk, o, true)) return rc;
+    r->storage = (uint32_t)w.storage;
     bool any_stop = false;
-    if (int rc = build_image(ctx, c, im, d, lb, &any_stop, r)) return rc;
-    cudaFree(d.chunk);
-    d.chunk = nullptr;
+    if (int rc = build_image(ctx, c, w, lb, &any_stop, r)) return rc;
     if (!any_stop) {
         r->wall_ms = now_ms() - t0;
         return NSAT_OK;
     }
-    GCK(cudaMalloc(&d.dest, L * 8));
-    GCK(cudaMalloc(&d.second, L * 8));
-    GCK(cudaMalloc(&d.best, 8));
     cudaStream_t st = ctx_stream(ctx);
     const int sms = ctx_sm_count(ctx);
-    cudaEvent_t e0, e1;
-    GCK(cudaEventCreate(&e0));
-    GCK(cudaEventCreate(&e1));
-    struct EvGuard {
-        cudaEvent_t a, b;
-        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
-    } eg{e0, e1};
     for (uint32_t stage = 0; stage < n; stage++) {
         for (uint32_t i = 0; i < P; i++) {
             const uint64_t start_i = (uint64_t)i * L;
-            if (int rc = image_to_device(ctx, im, (uint64_t)i * pbytes, pbytes, d.packed, st, r)) return rc;
-            KCK(nsat_greedy_unpack(d.packed, L, bits, d.dest, sms, st));
-            for (uint32_t j = 0; j < P; j++) {
-                if (j != i) {
-                    if (int rc = image_to_device(ctx, im, (uint64_t)j * pbytes, pbytes, d.packed, st, r)) return rc;
-                    KCK(nsat_greedy_unpack(d.packed, L, bits, d.second, sms, st));
-                } else {
-                    GCK(cudaMemcpyAsync(d.second, d.dest, L * 8, cudaMemcpyDeviceToDevice, st));
-                }
-                GCK(cudaEventRecord(e0, st));
-                KCK(nsat_greedy_join(d.dest, L, d.second, (uint64_t)j * L, L, n, sms, st));
-                GCK(cudaEventRecord(e1, st));
-                GCK(cudaEventSynchronize(e1));
-                float ms = 0;
-                GCK(cudaEventElapsedTime(&ms, e0, e1));
-                r->join_ms += ms;
-                r->joins++;
-            }
+            if (int rc = join_partition(ctx, w, n, P, L, i, r)) return rc;
             uint64_t best = ~0ull;
-            GCK(cudaMemcpyAsync(d.best, &best, 8, cudaMemcpyHostToDevice, st));
-            KCK(nsat_greedy_find(d.dest, start_i, L, n, o->unknowns, d.best, sms, st));
-            GCK(cudaMemcpyAsync(&best, d.best, 8, cudaMemcpyDeviceToHost, st));
+            GCK(cudaMemcpyAsync(w.best, &best, 8, cudaMemcpyHostToDevice, st));
+            KCK(nsat_greedy_find(w.dest, start_i, L, n, o->unknowns, w.best, sms, st));
+            GCK(cudaMemcpyAsync(&best, w.best, 8, cudaMemcpyDeviceToHost, st));
             GCK(cudaStreamSynchronize(st));
             if (best != ~0ull) {
                 uint64_t e = 0;
-                GCK(cudaMemcpy(&e, d.dest + (best - start_i), 8, cudaMemcpyDeviceToHost));
+                GCK(cudaMemcpy(&e, w.dest + (best - start_i), 8, cudaMemcpyDeviceToHost));
                 r->found = 1;
                 r->start = best;
                 r->end = e & ((1ull << n) - 1);
@@ -273,8 +372,13 @@ extern "C" int nsat_greedy_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_gree
                 r->wall_ms = now_ms() - t0;
                 return NSAT_OK;
             }
-            KCK(nsat_greedy_pack(d.dest, L, bits, d.packed, sms, st));
-            if (int rc = device_to_image(ctx, im, (uint64_t)i * pbytes, pbytes, d.packed, st, r)) return rc;
+            // write dest back to partition i of the image
+            if (w.storage == DEVICE) {
+                KCK(nsat_greedy_pack(w.dest, L, bits, w.dev_image + (uint64_t)i * pwords, sms, st));
+            } else {
+                KCK(nsat_greedy_pack(w.dest, L, bits, w.stage[0], sms, st));
+                if (int rc = store(ctx, w, (uint64_t)i * pbytes, pbytes, w.stage[0], st, r)) return rc;
+            }
             GCK(cudaStreamSynchronize(st));
         }
     }
@@ -290,25 +394,23 @@ extern "C" int nsat_greedy_image(nsat_ctx* ctx, nsat_circuit* c, uint32_t partit
     if (circ.outputs.size() != n + 1) return ctx_fail(ctx, NSAT_EINVAL, "SATOSTOP circuit needs n+1 outputs");
     nsat_greedy_opts o{};
     o.partitions = partitions;
+    o.file_prefix = file_prefix;
+    o.device_bytes = file_prefix ? 0 : 1;   // a host image unless a file is asked for
     uint32_t pbits = 0;
     if (int rc = check_opts(ctx, n, &o, &pbits)) return rc;
     const uint64_t total = packed_bytes(1ull << n, bits);
     if (nwords * 8 < total) return ctx_fail(ctx, NSAT_EINVAL, "image buffer too small");
     const uint32_t lb = std::min(pbits + 2, n - 10);
-    const uint64_t chunk = 1ull << (n - lb);
-    const uint64_t cbytes = packed_bytes(chunk, bits);
+    const uint64_t L = 1ull << (n - pbits), chunk = 1ull << (n - lb);
     GCK(cudaSetDevice(ctx_device(ctx)));
-    Image im;
-    if (int rc = open_image(ctx, im, total, cbytes, file_prefix)) return rc;
-    DevBufs d;
-    GCK(cudaMalloc(&d.chunk, chunk * 8));
-    GCK(cudaMalloc(&d.packed, cbytes));
+    Work w;
+    if (int rc = setup(ctx, w, n, L, chunk, &o, false)) return rc;
     nsat_greedy_result r{};
     bool any = false;
-    if (int rc = build_image(ctx, c, im, d, lb, &any, &r)) return rc;
-    if (im.host) {
-        memcpy(words, im.host, total);
-    } else if (!pread_all(im.fd, words, total, 0)) {
+    if (int rc = build_image(ctx, c, w, lb, &any, &r)) return rc;
+    if (w.storage == HOST) {
+        memcpy(words, w.host_image, total);
+    } else if (!pread_all(w.fd, words, total, 0)) {
         return ctx_fail(ctx, NSAT_EINVAL, "image file read failed");
     }
     return NSAT_OK;

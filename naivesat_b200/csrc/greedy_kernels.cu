@@ -5,8 +5,9 @@
 // space of n bits is n+1 bits (next | STOP << n) at bit i*(n+1) of a
 // little-endian u64 array; an entry may straddle two words.  Partitions hold
 // multiples of 64 entries, so every partition starts on a word boundary.
-// Joins run on unpacked u64 entries: unpacking and packing are one pass each
-// and make the joins race-free (packed entries share words).
+// The partition being updated is unpacked to u64 entries (an in-place join
+// on packed entries would race: entries share words); the partitions it
+// gathers from are read packed.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -62,6 +63,28 @@ __global__ void join_kernel(u64* __restrict__ dest, u64 count, const u64* __rest
     }
 }
 
+// The same join with `second` still packed (bits = n+1 per entry): the
+// gather reads the one or two words that hold the entry.
+__global__ void join_packed_kernel(u64* __restrict__ dest, u64 count, const u64* __restrict__ second, u64 start2,
+                                   u64 count2, u32 n) {
+    const u32 bits = n + 1;
+    const u64 state_mask = (1ull << n) - 1;
+    const u64 mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1);
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const u64 v = dest[i];
+        if ((v >> n) & 1ull) continue;
+        const u64 off = (v & state_mask) - start2;
+        if (off >= count2) continue;
+        const u64 b = off * bits;
+        const u64 w = b >> 6;
+        const u32 o = (u32)(b & 63);
+        u64 x = __ldg(second + w) >> o;
+        if (o + bits > 64) x |= __ldg(second + w + 1) << (64 - o);
+        dest[i] = x & mask;
+    }
+}
+
 // greedysatostop.rs MemImage::find_solution (482-507): the lowest unknown
 // start of the partition (low n-u bits zero) whose entry has STOP.
 __global__ void find_kernel(const u64* __restrict__ dest, u64 start, u64 count, u32 n, u32 unknowns,
@@ -103,6 +126,13 @@ extern "C" int nsat_greedy_pack(const uint64_t* in, uint64_t count, uint32_t bit
 extern "C" int nsat_greedy_join(uint64_t* dest, uint64_t count, const uint64_t* second, uint64_t start2,
                                 uint64_t count2, uint32_t n, int sms, cudaStream_t st) {
     join_kernel<<<grid_for(count, sms), 256, 0, st>>>((u64*)dest, count, (const u64*)second, start2, count2, n);
+    return cudaGetLastError() == cudaSuccess ? 0 : -4;
+}
+
+extern "C" int nsat_greedy_join_packed(uint64_t* dest, uint64_t count, const uint64_t* second_packed, uint64_t start2,
+                                       uint64_t count2, uint32_t n, int sms, cudaStream_t st) {
+    join_packed_kernel<<<grid_for(count, sms), 256, 0, st>>>((u64*)dest, count, (const u64*)second_packed, start2,
+                                                             count2, n);
     return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 

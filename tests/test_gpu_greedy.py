@@ -37,13 +37,17 @@ def test_image_layout_is_the_reference_memimage(ctx, tmp_path):
 @pytest.mark.parametrize("name,circ", list(circuits()))
 @pytest.mark.parametrize("partitions", [2, 4, 8])
 def test_partitioned_matches_oracle(ctx, name, circ, partitions):
+    """Device-resident image for the even partition counts' first unknowns
+    setting, host-spilled image (device budget of 1 byte) for the rest."""
     n = circ.n
     oc = O.Circuit(circ.n, circ.gates, circ.outputs)
     table = O.stop_table(oc)
     h = ctx.circuit(circ)
-    for u in sorted({n // 2, n - 2, n}):
+    for k, u in enumerate(sorted({n // 2, n - 2, n})):
         exp = O.greedy_partitioned(n, u, table, partitions)
-        got = h.greedy_partitioned(u, partitions)
+        spill = (k + partitions) % 2 == 1
+        got = h.greedy_partitioned(u, partitions, device_bytes=1 if spill else 0)
+        assert got["storage"] == (1 if spill else 0)
         if exp is None:
             assert not got["found"], (name, u)
             continue
@@ -53,14 +57,17 @@ def test_partitioned_matches_oracle(ctx, name, circ, partitions):
         assert O.stop_replay(oc, got["start"], 1 << (n + 1))[0] == got["end"]
 
 
-def test_file_image_equals_pinned(ctx, tmp_path):
+def test_device_host_and_file_images_agree(ctx, tmp_path):
     c = W.lfsr_stop(5, 16, 48)
     h = ctx.circuit(c)
     a = h.greedy_partitioned(8, 4)
-    b = h.greedy_partitioned(8, 4, file_prefix=str(tmp_path) + "/")
+    b = h.greedy_partitioned(8, 4, device_bytes=1)
+    f = h.greedy_partitioned(8, 4, file_prefix=str(tmp_path) + "/")
+    assert (a["storage"], b["storage"], f["storage"]) == (0, 1, 2)
     keys = ("found", "start", "end", "stage", "partition", "joins")
-    assert {k: a[k] for k in keys} == {k: b[k] for k in keys}
-    assert a["h2d_bytes"] == b["h2d_bytes"] and list(tmp_path.iterdir()) == []
+    assert {k: a[k] for k in keys} == {k: b[k] for k in keys} == {k: f[k] for k in keys}
+    assert a["h2d_bytes"] == 0 and b["h2d_bytes"] == f["h2d_bytes"] > 0
+    assert list(tmp_path.iterdir()) == []
 
 
 def test_partitioned_at_n20_against_oracle(ctx):
@@ -68,9 +75,10 @@ def test_partitioned_at_n20_against_oracle(ctx):
     oc = O.Circuit(c.n, c.gates, c.outputs)
     table = O.stop_table(oc)
     exp = O.greedy_partitioned(20, 12, table, 4)
-    got = ctx.circuit(c).greedy_partitioned(12, 4)
-    if exp is None:
-        assert not got["found"]
-    else:
-        assert (got["start"], got["end"], got["stage"], got["partition"]) == \
-            (exp["start"], exp["end"], exp["stage"], exp["partition"])
+    for budget in (0, 1):
+        got = ctx.circuit(c).greedy_partitioned(12, 4, device_bytes=budget)
+        if exp is None:
+            assert not got["found"]
+        else:
+            assert (got["start"], got["end"], got["stage"], got["partition"]) == \
+                (exp["start"], exp["end"], exp["stage"], exp["partition"])
