@@ -213,6 +213,39 @@ typedef struct {
 int nsat_stop_solve(nsat_ctx* ctx, nsat_table* t, const nsat_stop_opts* opts,
                     nsat_stop_result* res);
 
+/* ---- autotuning ----------------------------------------------------------
+ * Times the evaluator kernels of one circuit over a sample of its index
+ * space with candidate launch shapes -- threads per CTA, CTAs per SM the
+ * kernels are compiled for (the register budget), and CTA bits per launch
+ * against loop iterations per warp -- and keeps the fastest on the circuit
+ * handle: later nsat_sat_solve / nsat_qsat_solve calls on that handle use it.
+ * Answers are the same under every shape.  Candidates are compiled in
+ * parallel host threads.  With persist the choice is reused from / stored in
+ * the kernel cache directory, keyed by circuit, kind, quantifiers and GPU.
+ * No counterpart in the reference (its OpenCL group length is a flag). */
+typedef struct {
+    uint32_t kind;            /* 0 SAT, 1 QSAT */
+    uint32_t persist;         /* 1: reuse / store the choice in the kernel cache directory */
+    const uint8_t* quants;    /* QSAT: one per input, 1 = All */
+    double sample_ms;         /* device time measured per candidate (0 = 60 ms) */
+    uint32_t threads;         /* host compile threads (0 = hardware threads) */
+    uint32_t reserved;
+} nsat_tune_opts;
+
+typedef struct {
+    uint32_t block_threads, min_blocks, cta_bits_max;   /* the chosen shape */
+    uint32_t candidates;      /* shapes timed (0 when taken from the cache) */
+    uint32_t from_cache;
+    uint32_t reserved;
+    double best_rate;         /* assignments per second with the chosen shape */
+    double default_rate;      /* ... with the context's shape */
+    double tune_ms;           /* wall time of tuning */
+} nsat_tune_result;
+
+int nsat_autotune(nsat_ctx* ctx, nsat_circuit* c, const nsat_tune_opts* opts, nsat_tune_result* res);
+/* Forgets a circuit's tuned shapes: its solves use the context's options. */
+int nsat_autotune_reset(nsat_circuit* c);
+
 /* ---- partitioned greedysatostop (greedysatostop -p P [-x PREFIX]) -------
  * Replaces do_solve_with_cpu_builder_with_partitions
  * (greedysatostop.rs:692-837): the table is kept as a packed image of

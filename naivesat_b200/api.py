@@ -90,6 +90,17 @@ class GreedyResult(C.Structure):
                 ("wall_ms", C.c_double), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
 
+class TuneOpts(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("persist", C.c_uint32), ("quants", U8P), ("sample_ms", C.c_double),
+                ("threads", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("min_blocks", C.c_uint32), ("cta_bits_max", C.c_uint32),
+                ("candidates", C.c_uint32), ("from_cache", C.c_uint32), ("reserved", C.c_uint32),
+                ("best_rate", C.c_double), ("default_rate", C.c_double), ("tune_ms", C.c_double)]
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("arena_bytes", C.c_uint64), ("max_active", C.c_uint32), ("max_queue", C.c_uint32),
                 ("max_slice_tiles", C.c_uint32), ("first_slice_tiles", C.c_uint32),
@@ -127,6 +138,7 @@ EXPORTS = [
     "nsat_qsat_solve_noalloc", "nsat_server_create", "nsat_server_destroy", "nsat_server_submit",
     "nsat_server_step", "nsat_server_poll", "nsat_server_stats", "nsat_gen_random_dag",
     "nsat_gen_lfsr_stop", "nsat_server_program_check", "nsat_greedy_solve", "nsat_greedy_image",
+    "nsat_autotune", "nsat_autotune_reset",
 ]
 
 _lib = None
@@ -173,6 +185,8 @@ def lib():
         L.nsat_table_bytes.restype = C.c_uint64
         L.nsat_stop_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(StopOpts), C.POINTER(StopResult)]
         L.nsat_probe_lop3_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.nsat_autotune.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(TuneOpts), C.POINTER(TuneResult)]
+        L.nsat_autotune_reset.argtypes = [C.c_void_p]
         L.nsat_greedy_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(GreedyOpts), C.POINTER(GreedyResult)]
         L.nsat_greedy_image.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_char_p, U64P, C.c_uint64]
         L.nsat_server_create.argtypes = [C.c_void_p, C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]
@@ -336,6 +350,19 @@ class CircuitHandle:
 
     def stop_table(self, want_steps=False):
         return Table(self, want_steps)
+
+    def autotune(self, kind="sat", quants=None, persist=False, sample_ms=0.0, threads=0):
+        """nsat_autotune: times candidate launch shapes on a sample of this
+        circuit's index space and keeps the fastest for later solves."""
+        q = _quants_array(quants, self.n) if quants is not None else None
+        o = TuneOpts(0 if kind == "sat" else 1, 1 if persist else 0,
+                     q.ctypes.data_as(U8P) if q is not None else None, sample_ms, threads, 0)
+        r = TuneResult()
+        self.ctx._check(lib().nsat_autotune(self.ctx.h, self.h, C.byref(o), C.byref(r)), "autotune")
+        return {f: getattr(r, f) for f, _ in TuneResult._fields_ if f != "reserved"}
+
+    def autotune_reset(self):
+        lib().nsat_autotune_reset(self.h)
 
     def greedy_partitioned(self, unknowns, partitions, file_prefix=None, device_bytes=0):
         """greedysatostop -p: the table as a packed image (device memory when

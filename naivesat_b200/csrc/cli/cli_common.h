@@ -212,6 +212,25 @@ inline nsat_ctx* open_ctx(int device, const Args& a) {
     return ctx;
 }
 
+// With NSAT_AUTOTUNE set in the environment, the circuit's launch shape is
+// tuned before solving (nsat_autotune, remembered in the kernel cache
+// directory, so the cost is paid once per circuit and GPU).  Answers do not
+// depend on it.
+inline int maybe_autotune(nsat_ctx* ctx, nsat_circuit* c, uint32_t kind, const uint8_t* quants) {
+    if (!getenv("NSAT_AUTOTUNE")) return NSAT_OK;
+    nsat_tune_opts o{};
+    o.kind = kind;
+    o.persist = 1;
+    o.quants = quants;
+    nsat_tune_result r{};
+    const int rc = nsat_autotune(ctx, c, &o, &r);
+    if (rc == NSAT_OK && getenv("NSAT_VERBOSE"))
+        fprintf(stderr, "[nsat] autotune: %u threads, %u CTAs/SM, %u CTA bits (%s, %.2fx)\n", r.block_threads,
+                r.min_blocks, r.cta_bits_max, r.from_cache ? "cached" : "measured",
+                r.default_rate > 0 ? r.best_rate / r.default_rate : 0.0);
+    return rc;
+}
+
 inline void check(nsat_ctx* ctx, int rc, const char* what) {
     if (rc != NSAT_OK) die(std::string(what) + ": " + nsat_strerror(rc) + " " + nsat_last_error(ctx), 1);
 }

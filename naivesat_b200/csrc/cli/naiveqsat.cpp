@@ -63,6 +63,7 @@ int main(int argc, char** argv) {
             nsat_ctx* ctx = open_ctx(et.devices[i], a);
             nsat_circuit* c = nullptr;
             int rc = nsat_circuit_new(ctx, &L.d, &c);
+            if (rc == NSAT_OK) rc = maybe_autotune(ctx, c, 1, quants.data());
             if (rc == NSAT_OK) {
                 nsat_qsat_opts o{};
                 o.chunk_bits = chunk_bits;

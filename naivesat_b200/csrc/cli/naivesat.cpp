@@ -55,6 +55,7 @@ int main(int argc, char** argv) {
             nsat_ctx* ctx = open_ctx(et.devices[i], a);
             nsat_circuit* c = nullptr;
             int rc = nsat_circuit_new(ctx, &L.d, &c);
+            if (rc == NSAT_OK) rc = maybe_autotune(ctx, c, 0, nullptr);
             if (rc == NSAT_OK) {
                 nsat_sat_opts o{};
                 o.find_all = 0;

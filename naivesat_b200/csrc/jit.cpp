@@ -218,4 +218,8 @@ int jit_get(int device, const std::string& src, const std::vector<std::string>& 
     return 0;
 }
 
+std::string jit_cache_dir() { return cache_dir(); }
+
+uint64_t jit_fnv(const std::string& s) { return fnv(s); }
+
 }  // namespace nsat

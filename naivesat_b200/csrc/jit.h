@@ -47,6 +47,13 @@ int jit_get(int device, const std::string& src, const std::vector<std::string>& 
 // (ptxas resource usage) and the compile time.
 int jit_compile_only(const std::string& src, std::string* log, double* ms, std::string* err);
 
+// Directory of the on-disk kernel cache (NSAT_JIT_CACHE, else the user's
+// cache directory).
+std::string jit_cache_dir();
+
+// FNV-1a 64 of a byte string (cache keys).
+uint64_t jit_fnv(const std::string& s);
+
 // Drops every cached module (call with the device's context current).
 void jit_clear();
 

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -65,10 +67,19 @@ struct nsat_ctx {
     NsatJoinState* h_join = nullptr;
 };
 
+// Launch shape of the evaluator kernels: threads per CTA, CTAs per SM the
+// kernels are compiled for, and the cap on CTA bits per launch (the rest of
+// a launch's bits are loop iterations per warp).  0 = the context's choice.
+struct Shape {
+    uint32_t block_threads = 0, min_blocks = 0, cb_max = 0;
+};
+
 struct nsat_circuit {
     nsat_ctx* ctx = nullptr;
     Circuit circ;
     std::map<std::string, LutNet> nets;
+    Shape tuned;                 // set by nsat_autotune (per kind)
+    Shape tuned_qsat;
 };
 
 struct nsat_table {
@@ -135,8 +146,18 @@ const LutNet& get_net(nsat_circuit* c, const std::vector<uint32_t>& which) {
     return c->nets[key] = map_luts(c->circ, which, c->ctx->opts.no_optimize != 0);
 }
 
+// The shape a solve uses: the circuit's tuned one when set, else the
+// context's options.
+Shape effective_shape(const nsat_ctx* ctx, const Shape& tuned) {
+    Shape s;
+    s.block_threads = tuned.block_threads ? tuned.block_threads : ctx->opts.block_threads;
+    s.min_blocks = tuned.block_threads ? tuned.min_blocks : ctx->opts.min_blocks;
+    s.cb_max = tuned.cb_max;
+    return s;
+}
+
 // Splits the launch's C enumeration bits into lane(5)+warp-lane(5)+IT+WB+CB.
-void choose_shape(uint32_t C, uint32_t block_threads, KernelConfig* kc) {
+void choose_shape(uint32_t C, uint32_t block_threads, KernelConfig* kc, uint32_t cb_max = 0) {
     uint32_t wb = 3;
     if (block_threads) {
         wb = 0;
@@ -144,7 +165,7 @@ void choose_shape(uint32_t C, uint32_t block_threads, KernelConfig* kc) {
     }
     if (wb > C - 10) wb = C - 10;
     uint32_t rest = C - 10 - wb;
-    uint32_t cb = std::min<uint32_t>(rest, 12);
+    uint32_t cb = std::min<uint32_t>(rest, cb_max ? cb_max : 12);
     uint32_t it = rest - cb;
     if (it > 10) { it = 10; cb = rest - 10; }
     kc->wb = wb; kc->it = it; kc->cb = cb; kc->c = C;
@@ -256,8 +277,8 @@ struct SatPlan {
     u128 bp = 0, ep = 0;   // range in the padded index space
 };
 
-int plan_sat(uint32_t n, const nsat_sat_opts& o, uint32_t block_threads, uint32_t min_blocks, SatPlan* pl,
-             std::string* err) {
+int plan_sat(uint32_t n, const nsat_sat_opts& o, const Shape& sh, SatPlan* pl, std::string* err) {
+    const uint32_t block_threads = sh.block_threads, min_blocks = sh.min_blocks;
     const uint32_t d = n < 15 ? 15 - n : 0;     // dummy low bits for tiny circuits
     const uint32_t np = n + d;
     if (np > 128) { *err = "too many inputs"; return NSAT_EUNSUPPORTED; }
@@ -279,7 +300,7 @@ int plan_sat(uint32_t n, const nsat_sat_opts& o, uint32_t block_threads, uint32_
     kc.nb = np;
     kc.in_of_bit.resize(np);
     for (uint32_t p = 0; p < np; p++) kc.in_of_bit[p] = p < d ? -1 : (int)(p - d);
-    choose_shape(C, block_threads, &kc);
+    choose_shape(C, block_threads, &kc, sh.cb_max);
     kc.minb = min_blocks ? min_blocks : default_min_blocks(kc);
     pl->d = d; pl->C = C; pl->bp = bp; pl->ep = ep;
     return NSAT_OK;
@@ -295,8 +316,8 @@ struct QsatPlan {
 };
 
 int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint32_t chunk_bits,
-              uint32_t block_threads, uint32_t min_blocks, uint32_t prefix_bits, QsatPlan* pl,
-              std::string* err) {
+              const Shape& sh, uint32_t prefix_bits, QsatPlan* pl, std::string* err) {
+    const uint32_t block_threads = sh.block_threads, min_blocks = sh.min_blocks;
     if (quants_in.size() != n || n == 0) { *err = "quantifier count differs from inputs"; return NSAT_EINVAL; }
     if (prefix_bits >= n) { *err = "prefix must leave at least one free input"; return NSAT_EINVAL; }
     const uint32_t d = n < 15 ? 15 - n : 0;
@@ -324,7 +345,7 @@ int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint
         int in = (int)(np - 1 - p);
         kc.in_of_bit[p] = (data || in >= (int)n) ? -1 : in;
     }
-    choose_shape(C, block_threads, &kc);
+    choose_shape(C, block_threads, &kc, sh.cb_max);
     kc.minb = min_blocks ? min_blocks : default_min_blocks(kc);
     kc.m = std::min<uint32_t>(m, 127);
     kc.q0all = q[s] != 0;
@@ -531,7 +552,7 @@ extern "C" int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opt
     if (opts) o = *opts;
     SatPlan plan;
     std::string perr;
-    if (int rc = plan_sat(c->circ.n, o, ctx->opts.block_threads, ctx->opts.min_blocks, &plan, &perr)) return fail(ctx, rc, perr);
+    if (int rc = plan_sat(c->circ.n, o, effective_shape(ctx, c->tuned), &plan, &perr)) return fail(ctx, rc, perr);
     const KernelConfig& kc = plan.kc;
     const uint32_t d = plan.d, C = plan.C;
     const u128 bp = plan.bp, ep = plan.ep;
@@ -602,8 +623,8 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     const uint32_t n = data ? n_items_bits : c->circ.n;
     QsatPlan plan;
     std::string perr;
-    if (int rc = plan_qsat(n, quants_in, data, chunk_bits, ctx->opts.block_threads, ctx->opts.min_blocks,
-                           prefix_bits, &plan, &perr))
+    const Shape sh = data ? effective_shape(ctx, Shape()) : effective_shape(ctx, c->tuned_qsat);
+    if (int rc = plan_qsat(n, quants_in, data, chunk_bits, sh, prefix_bits, &plan, &perr))
         return fail(ctx, rc, perr);
     if (prefix_bits < 64 && (prefix >> prefix_bits) != 0) return fail(ctx, NSAT_EINVAL, "prefix wider than prefix_bits");
     const KernelConfig& kc = plan.kc;
@@ -980,8 +1001,9 @@ extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quan
     Circuit c = from_desc(desc);
     if (!c.validate().empty()) return NSAT_EINVAL;
     const bool raw = opts && opts->no_optimize;
-    const uint32_t bt = opts ? opts->block_threads : 0;
-    const uint32_t mb = opts ? opts->min_blocks : 0;
+    Shape sh;
+    sh.block_threads = opts ? opts->block_threads : 0;
+    sh.min_blocks = opts ? opts->min_blocks : 0;
     KernelConfig kc;
     std::vector<uint32_t> which{0};
     std::string err;
@@ -990,14 +1012,14 @@ extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quan
         SatPlan pl;
         nsat_sat_opts so{};
         so.find_all = 1;
-        rc = plan_sat(c.n, so, bt, mb, &pl, &err);
+        rc = plan_sat(c.n, so, sh, &pl, &err);
         kc = pl.kc;
     } else if (kind == 1) {
         if (!quants) return NSAT_EINVAL;
         std::vector<uint8_t> q(quants, quants + c.n);
         for (auto& v : q) v = v ? 1 : 0;
         QsatPlan pl;
-        rc = plan_qsat(c.n, q, false, 0, bt, mb, 0, &pl, &err);
+        rc = plan_qsat(c.n, q, false, 0, sh, 0, &pl, &err);
         kc = pl.kc;
     } else {
         rc = plan_table(c, false, &kc, &err);
@@ -1033,5 +1055,230 @@ extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quan
         b = (b == std::string::npos) ? clog.rfind(' ', p - 2) : b + 1;
         info->spill_bytes = atoi(clog.c_str() + b);
     }
+    return NSAT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuning
+
+namespace {
+
+struct Candidate {
+    Shape sh;
+    double rate = 0;
+};
+
+// Assignments per second of the circuit's solve under shape sh: one warm-up
+// solve, then solves until sample_ms of device time has accumulated.
+int measure_shape(nsat_ctx* ctx, nsat_circuit* c, uint32_t kind, const uint8_t* quants, const Shape& sh,
+                  double sample_ms, double* rate) {
+    Shape& slot = kind == 0 ? c->tuned : c->tuned_qsat;
+    const Shape keep = slot;
+    slot = sh;
+    if (!slot.block_threads) slot.block_threads = 256;   // an explicit shape, never "unset"
+    double dev = 0, items = 0;
+    int rc = NSAT_OK;
+    for (int run = 0; run < 1000 && rc == NSAT_OK; run++) {
+        double ms = 0, it = 0;
+        if (kind == 0) {
+            nsat_sat_opts o{};
+            o.find_all = 1;
+            const uint32_t n = c->circ.n;
+            const uint32_t bits = std::min<uint32_t>(n, 35);
+            const u128 end = (u128)1 << bits;
+            o.end_lo = (uint64_t)end;
+            o.end_hi = (uint64_t)(end >> 64);
+            nsat_sat_result r{};
+            rc = nsat_sat_solve(ctx, c, &o, &r);
+            ms = r.device_ms;
+            it = (double)r.scanned_lo + 18446744073709551616.0 * (double)r.scanned_hi;
+        } else {
+            // at most 2^35 items: the sub-problem under an all-zero prefix
+            nsat_qsat_opts qo{};
+            qo.prefix_bits = c->circ.n > 35 ? c->circ.n - 35 : 0;
+            nsat_qsat_result r{};
+            rc = nsat_qsat_solve(ctx, c, quants, &qo, &r);
+            ms = r.device_ms;
+            it = (double)r.scanned;
+        }
+        if (run == 0) continue;      // warm-up: module load, first-launch costs
+        dev += ms;
+        items += it;
+        if (dev >= sample_ms && run >= 2) break;
+    }
+    slot = keep;
+    if (rc) return rc;
+    *rate = dev > 0 ? items / (dev * 1e-3) : 0;
+    return NSAT_OK;
+}
+
+// Compiles the candidates' kernels in parallel host threads (NVRTC is
+// thread-safe; modules load into the device's primary context).
+void precompile(nsat_ctx* ctx, nsat_circuit* c, uint32_t kind, const std::vector<uint8_t>& q,
+                const std::vector<Candidate>& cands, uint32_t threads) {
+    std::vector<std::string> srcs;
+    const std::vector<uint32_t> out0{0};
+    const LutNet& net = get_net(c, out0);
+    for (const Candidate& cd : cands) {
+        Shape sh = cd.sh;
+        if (!sh.block_threads) sh.block_threads = 256;
+        std::string err;
+        KernelConfig kc;
+        if (kind == 0) {
+            SatPlan pl;
+            nsat_sat_opts o{};
+            o.find_all = 1;
+            if (plan_sat(c->circ.n, o, sh, &pl, &err)) continue;
+            kc = pl.kc;
+        } else {
+            QsatPlan pl;
+            if (plan_qsat(c->circ.n, q, false, 0, sh, 0, &pl, &err)) continue;
+            kc = pl.kc;
+        }
+        srcs.push_back(generate_source(kc, net));
+    }
+    const char* name = kind == 0 ? "nsat_sat" : "nsat_qsat";
+    const int dev = ctx->device;
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        cudaSetDevice(dev);
+        cudaFree(nullptr);
+        for (size_t i = next++; i < srcs.size(); i = next++) {
+            std::shared_ptr<JitModule> m;
+            std::string err;
+            jit_get(dev, srcs[i], {name}, false, &m, &err);   // failures resurface when measured
+        }
+    };
+    const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t nt = std::min<uint32_t>(threads ? threads : hw, (uint32_t)srcs.size());
+    std::vector<std::thread> pool;
+    for (uint32_t t = 0; t + 1 < nt; t++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+}
+
+std::string tune_key(nsat_ctx* ctx, nsat_circuit* c, uint32_t kind, const uint8_t* quants) {
+    std::string k = "tune1|" + std::to_string(kind) + "|" + std::to_string(c->circ.n) + "|";
+    for (const Gate& g : c->circ.gates) k += std::to_string(g.func) + "," + std::to_string(g.i0) + "," + std::to_string(g.i1) + ";";
+    k += "|";
+    for (const Output& o : c->circ.outputs) k += std::to_string(o.wire) + (o.neg ? "n;" : ";");
+    if (kind == 1 && quants)
+        for (uint32_t i = 0; i < c->circ.n; i++) k += quants[i] ? 'A' : 'E';
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess)
+        k += std::string("|") + prop.name + "|" + std::to_string(prop.multiProcessorCount);
+    k += "|" + std::to_string(ctx->opts.no_optimize);
+    char hex[32];
+    snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)jit_fnv(k));
+    return jit_cache_dir() + "/tune_" + hex + ".txt";
+}
+
+}  // namespace
+
+extern "C" int nsat_autotune(nsat_ctx* ctx, nsat_circuit* c, const nsat_tune_opts* opts, nsat_tune_result* res) {
+    if (!ctx || !c || !opts || !res || opts->kind > 1) return NSAT_EINVAL;
+    if (opts->kind == 1 && !opts->quants) return NSAT_EINVAL;
+    memset(res, 0, sizeof(*res));
+    const double t0 = now_ms();
+    if (int rc = set_device(ctx)) return rc;
+    const uint32_t kind = opts->kind;
+    std::vector<uint8_t> q;
+    if (kind == 1) {
+        q.assign(opts->quants, opts->quants + c->circ.n);
+        for (auto& v : q) v = v ? 1 : 0;
+    }
+    const double sample = opts->sample_ms > 0 ? opts->sample_ms : 60.0;
+    Shape& slot = kind == 0 ? c->tuned : c->tuned_qsat;
+    const std::string path = tune_key(ctx, c, kind, opts->quants);
+    if (opts->persist) {
+        FILE* f = fopen(path.c_str(), "r");
+        if (f) {
+            unsigned bt = 0, mb = 0, cb = 0;
+            double rate = 0, drate = 0;
+            const int got = fscanf(f, "%u %u %u %lf %lf", &bt, &mb, &cb, &rate, &drate);
+            fclose(f);
+            if (got == 5 && bt) {
+                slot.block_threads = bt; slot.min_blocks = mb; slot.cb_max = cb;
+                res->block_threads = bt; res->min_blocks = mb; res->cta_bits_max = cb;
+                res->best_rate = rate; res->default_rate = drate;
+                res->from_cache = 1;
+                res->tune_ms = now_ms() - t0;
+                return NSAT_OK;
+            }
+        }
+    }
+    // stage 1: threads per CTA x resident warps per SM (register budget)
+    std::vector<Candidate> st1;
+    for (uint32_t bt : {128u, 256u, 512u})
+        for (uint32_t warps : {16u, 24u, 32u}) {
+            Candidate cd;
+            cd.sh.block_threads = bt;
+            cd.sh.min_blocks = std::max(1u, warps / (bt / 32));
+            bool dup = false;
+            for (const Candidate& o : st1) dup |= o.sh.block_threads == bt && o.sh.min_blocks == cd.sh.min_blocks;
+            if (!dup) st1.push_back(cd);
+        }
+    precompile(ctx, c, kind, q, st1, opts->threads);
+    // the context's own shape: first as a warm-up long enough for the clocks
+    // to leave idle (the GPU sat idle while the host compiled), then timed
+    const Shape def = effective_shape(ctx, Shape());
+    double default_rate = 0, warm = 0;
+    if (int rc = measure_shape(ctx, c, kind, opts->quants, def, std::max(250.0, sample), &warm)) return rc;
+    if (int rc = measure_shape(ctx, c, kind, opts->quants, def, sample, &default_rate)) return rc;
+    Candidate best;
+    for (Candidate& cd : st1) {
+        if (int rc = measure_shape(ctx, c, kind, opts->quants, cd.sh, sample, &cd.rate)) return rc;
+        res->candidates++;
+        if (cd.rate > best.rate) best = cd;
+    }
+    // stage 2: CTA bits per launch (the rest are iterations per warp)
+    std::vector<Candidate> st2;
+    for (uint32_t cb : {8u, 10u, 14u, 16u}) {
+        Candidate cd = best;
+        cd.sh.cb_max = cb;
+        st2.push_back(cd);
+    }
+    precompile(ctx, c, kind, q, st2, opts->threads);
+    for (Candidate& cd : st2) {
+        if (int rc = measure_shape(ctx, c, kind, opts->quants, cd.sh, sample, &cd.rate)) return rc;
+        res->candidates++;
+        if (cd.rate > best.rate * 1.01) best = cd;     // keep the default CTA cap unless clearly faster
+    }
+    // the winner and the default once more, back to back
+    double again = 0, def_again = 0;
+    if (int rc = measure_shape(ctx, c, kind, opts->quants, best.sh, sample, &again)) return rc;
+    if (int rc = measure_shape(ctx, c, kind, opts->quants, def, sample, &def_again)) return rc;
+    best.rate = std::max(best.rate, again);
+    default_rate = std::max(default_rate, def_again);
+    if (best.rate < default_rate) {   // the default shape held up
+        best.sh = def;
+        best.rate = default_rate;
+    }
+    slot = best.sh;
+    if (!slot.block_threads) slot.block_threads = 256;
+    if (!slot.cb_max) slot.cb_max = 12;
+    res->block_threads = slot.block_threads;
+    res->min_blocks = slot.min_blocks;
+    res->cta_bits_max = slot.cb_max;
+    res->best_rate = best.rate;
+    res->default_rate = default_rate;
+    if (opts->persist) {
+        const std::string tmp = path + ".tmp";
+        FILE* f = fopen(tmp.c_str(), "w");
+        if (f) {
+            fprintf(f, "%u %u %u %.6e %.6e\n", slot.block_threads, slot.min_blocks, slot.cb_max, best.rate,
+                    default_rate);
+            fclose(f);
+            rename(tmp.c_str(), path.c_str());
+        }
+    }
+    res->tune_ms = now_ms() - t0;
+    return NSAT_OK;
+}
+
+extern "C" int nsat_autotune_reset(nsat_circuit* c) {
+    if (!c) return NSAT_EINVAL;
+    c->tuned = Shape();
+    c->tuned_qsat = Shape();
     return NSAT_OK;
 }

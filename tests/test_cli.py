@@ -14,9 +14,9 @@ BIN = os.path.join(ROOT, "naivesat_b200", "bin")
 TOOLS = ["naivesat", "naiveqsat", "naivesatostop", "greedysatostop"]
 
 
-def run(tool, *args, check=False):
+def run(tool, *args, check=False, env=None):
     p = subprocess.run([os.path.join(BIN, tool)] + [str(a) for a in args], capture_output=True,
-                       text=True, timeout=600)
+                       text=True, timeout=600, env=dict(os.environ, **env) if env else None)
     if check:
         assert p.returncode == 0, p.stdout + p.stderr
     return p
@@ -123,3 +123,22 @@ def test_greedy_partitions_cli(tmp_path):
     assert list(spill.iterdir()) == []
     p = run("greedysatostop", path, 8, "-p", "3")
     assert p.returncode == 101 and "power of 2" in p.stderr + p.stdout
+
+
+@gpu
+def test_autotuned_clis_answer_the_same(tmp_path):
+    """NSAT_AUTOTUNE=1 tunes the launch shape (kept in the kernel cache
+    directory); the answer lines do not change."""
+    env = {"NSAT_AUTOTUNE": "1", "NSAT_JIT_CACHE": str(tmp_path / "cache")}
+    c = W.config("c0")
+    path = write(tmp_path, c, "c0")
+    plain = run("naivesat", path, "-t", "opencl:0", check=True).stdout
+    tuned = run("naivesat", path, "-t", "opencl:0", check=True, env=env).stdout
+    line = [x for x in plain.splitlines() if x.startswith(("Found Input", "Unsatisfiable"))]
+    assert line and line[0] in tuned
+    assert any(f.startswith("tune_") for f in os.listdir(tmp_path / "cache"))
+    q = write(tmp_path, W.config("c2a"), "a")
+    plain = run("naiveqsat", q, "-t", "opencl:0", check=True).stdout
+    tuned = run("naiveqsat", q, "-t", "opencl:0", check=True, env=env).stdout
+    res = [x for x in plain.splitlines() if x.startswith("Result:")]
+    assert res and res[0] in tuned
