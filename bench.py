@@ -229,6 +229,18 @@ class QsatWorkload:
         return (1 << self.circ.n) * self.circ.num_gates / dt, "full oracle solve (%.1f s)" % dt
 
 
+def gather_roofline(ctx, log2_table, gathers, stream_bytes, ms, hbm_gbs):
+    """A join is one random gather per entry plus streaming reads/writes:
+    its ceiling is gathers / (measured random-gather rate over a table of the
+    same size) + stream_bytes / (measured copy bandwidth)."""
+    g = ctx.gather_peak(min(34, max(10, log2_table)))
+    t = gathers / g + stream_bytes / (hbm_gbs * 1e9)
+    return {"gathers_per_s_peak": g, "table_log2": log2_table, "ceiling_ms": t * 1e3, "achieved_ms": ms,
+            "frac": t * 1e3 / ms,
+            "note": "gather peak: nsat_probe_gather_peak, independent random 8-byte loads over a table of "
+                    "2^table_log2 u64; streaming at the measured copy bandwidth"}
+
+
 class StopWorkload:
     """SATOSTOP: table build + synchronous doubling, both on the device."""
     metric = "join GB/s"
@@ -278,10 +290,13 @@ class StopWorkload:
     def roofline(self, world, dev_ms_per_step, peak_lop3, probe_mhz):
         peak, src = measured_hbm_gbs()
         ach = self.join_bytes() / (self.join_ms * 1e-3) / 1e9
-        return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": None, "peak_source": "%s hbm_gbs (MEASURED_PEAKS.json)" % src,
-                "kernel": "join_round", "algorithmic_bytes_per_entry_round": 3 * self.eb,
-                "rounds": self.rounds, "join_ms": self.join_ms, "build_ms": self.build_ms}
+        out = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+               "traffic": None, "peak_source": "%s hbm_gbs (MEASURED_PEAKS.json)" % src,
+               "kernel": "join_round", "algorithmic_bytes_per_entry_round": 3 * self.eb,
+               "rounds": self.rounds, "join_ms": self.join_ms, "build_ms": self.build_ms}
+        out["gather_roofline"] = gather_roofline(self.ctx, self.circ.n, (1 << self.circ.n) * self.rounds,
+                                                 (1 << self.circ.n) * self.rounds * 2 * self.eb, self.join_ms, peak)
+        return out
 
     def cpu(self, threads, target_s=12.0):
         from oracle import oracle as O
@@ -351,6 +366,11 @@ class StopPartWorkload:
                "storage": ["device", "pinned host", "file"][r["storage"]]}
         if self.spill:
             out["pcie_gbs"] = (r["h2d_bytes"] + r["d2h_bytes"]) / (r["wall_ms"] * 1e-3) / 1e9
+        L = 1 << (self.n - 2)
+        # per join: L/P gathers from the packed partition (~L*(n+1)/8 bytes, i.e. 2^(n-3) u64 of table),
+        # 8 B read per entry, 8 B written per gathered entry
+        out["gather_roofline"] = gather_roofline(self.ctx, self.n - 3, r["joins"] * L / self.P,
+                                                 r["joins"] * (8 * L + 8 * L / self.P), r["join_ms"], peak)
         return out
 
     def cpu(self, threads, target_s=12.0):
@@ -667,9 +687,10 @@ def run_serving(args, world, rank, local):
                      "peak_source": "measured lop3.b32 chain microbenchmark on this GPU (%.0f MHz)" % probe_mhz},
         "cpu_baseline": cpu,
         "e2e": {"value": sat_sum["solves_per_s"], "unit": "solves/s",
-                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "h2d_bytes_per_step": st_sat["h2d_bytes"] / len(reqs),
+                "d2h_bytes_per_step": st_sat["d2h_bytes"] / len(reqs),
                 "note": "the server runs end to end: circuits arrive as host arrays, programs and epoch tables "
-                        "are copied in, results copied out"},
+                        "are copied in, results copied out; bytes per request from the server's counters"},
         "gpu_launches": st_sat["launches"],
         "clocks": clk,
     }

@@ -341,6 +341,7 @@ typedef struct {
     uint64_t arena_used, arena_bytes;
     uint32_t graph_slots, grid;
     uint64_t launches;          /* kernels launched: epoch graphs and join rounds */
+    uint64_t h2d_bytes, d2h_bytes;   /* host<->device copies issued: programs, epoch tables, results */
 } nsat_server_stats_t;
 
 int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out);
@@ -401,6 +402,10 @@ int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quants, int kin
 /* Measures this device's 32-bit LOP3 issue rate with a chain microbenchmark
  * (independent lop3.b32 chains, no memory traffic): thread-instructions/s. */
 int nsat_probe_lop3_peak(nsat_ctx* ctx, double* lop3_per_s, double* sm_clock_mhz);
+/* Random 8-byte gathers per second from a device table of 2^log2_entries
+ * u64 (10..34), addresses independent of the data: the ceiling of the
+ * SATOSTOP joins' gathers (measurement aid; allocates and frees the table). */
+int nsat_probe_gather_peak(nsat_ctx* ctx, uint32_t log2_entries, double* gathers_per_s);
 
 #ifdef __cplusplus
 }

@@ -126,7 +126,8 @@ class JobResult(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("epochs", C.c_uint64), ("device_ms", C.c_double), ("active", C.c_uint32),
                 ("queued", C.c_uint32), ("arena_used", C.c_uint64), ("arena_bytes", C.c_uint64),
-                ("graph_slots", C.c_uint32), ("grid", C.c_uint32), ("launches", C.c_uint64)]
+                ("graph_slots", C.c_uint32), ("grid", C.c_uint32), ("launches", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
 
 
 EXPORTS = [
@@ -138,7 +139,7 @@ EXPORTS = [
     "nsat_qsat_solve_noalloc", "nsat_server_create", "nsat_server_destroy", "nsat_server_submit",
     "nsat_server_step", "nsat_server_poll", "nsat_server_stats", "nsat_gen_random_dag",
     "nsat_gen_lfsr_stop", "nsat_server_program_check", "nsat_greedy_solve", "nsat_greedy_image",
-    "nsat_autotune", "nsat_autotune_reset",
+    "nsat_autotune", "nsat_autotune_reset", "nsat_probe_gather_peak",
 ]
 
 _lib = None
@@ -185,6 +186,7 @@ def lib():
         L.nsat_table_bytes.restype = C.c_uint64
         L.nsat_stop_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(StopOpts), C.POINTER(StopResult)]
         L.nsat_probe_lop3_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.nsat_probe_gather_peak.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]
         L.nsat_autotune.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(TuneOpts), C.POINTER(TuneResult)]
         L.nsat_autotune_reset.argtypes = [C.c_void_p]
         L.nsat_greedy_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(GreedyOpts), C.POINTER(GreedyResult)]
@@ -271,6 +273,12 @@ class Context:
     def circuit(self, circ):
         """Loads a workloads.Circuit (or anything with n, gates, outputs)."""
         return CircuitHandle(self, circ.n, circ.gates, circ.outputs)
+
+    def gather_peak(self, log2_entries):
+        """Random 8-byte gathers per second from a table of 2^log2_entries u64."""
+        g = C.c_double()
+        self._check(lib().nsat_probe_gather_peak(self.h, log2_entries, C.byref(g)), "probe_gather_peak")
+        return g.value
 
     def lop3_peak(self):
         r, mhz = C.c_double(), C.c_double()

@@ -989,6 +989,41 @@ extern "C" int nsat_probe_lop3_peak(nsat_ctx* ctx, double* lop3_per_s, double* s
     return NSAT_OK;
 }
 
+extern "C" int nsat_probe_gather_peak(nsat_ctx* ctx, uint32_t log2_entries, double* gathers_per_s) {
+    if (!ctx || !gathers_per_s || log2_entries < 10 || log2_entries > 34) return NSAT_EINVAL;
+    if (int rc = set_device(ctx)) return rc;
+    const int blocks = ctx->sm_count * 8;
+    const uint64_t items = 1ull << 30;
+    uint64_t* table = nullptr;
+    uint64_t* out = nullptr;
+    if (cudaMalloc(&table, (size_t)8 << log2_entries) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, NSAT_ENOMEM, "gather probe table does not fit");
+    }
+    if (cudaMalloc(&out, (size_t)blocks * 256 * 8) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(table);
+        return fail(ctx, NSAT_ENOMEM, "gather probe output");
+    }
+    double best = 0;
+    int rc = NSAT_OK;
+    if (cudaMemsetAsync(table, 0x5a, (size_t)8 << log2_entries, ctx->stream) != cudaSuccess) rc = NSAT_ECUDA;
+    for (int rep = 0; rep < 4 && rc == NSAT_OK; rep++) {
+        cudaEventRecord(ctx->ev0[0], ctx->stream);
+        if (nsat_launch_gather_probe(table, log2_entries, items, out, blocks, ctx->stream)) { rc = NSAT_ECUDA; break; }
+        cudaEventRecord(ctx->ev1[0], ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = NSAT_ECUDA; break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev0[0], ctx->ev1[0]);
+        if (rep > 0 && ms > 0) best = std::max(best, (double)items / (ms * 1e-3));   // rep 0 warms up
+    }
+    cudaFree(table);
+    cudaFree(out);
+    if (rc) return fail(ctx, rc, "gather probe failed");
+    *gathers_per_s = best;
+    return NSAT_OK;
+}
+
 // ---------------------------------------------------------------------------
 // build check (no device needed)
 

@@ -263,6 +263,7 @@ struct nsat_server {
     NsatJoinState* d_join = nullptr;
     NsatJoinState* h_join = nullptr;
     uint64_t epochs = 0, launches = 0;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic the server issued
     double device_ms = 0;
 
     ~nsat_server() {
@@ -366,6 +367,7 @@ int admit(nsat_server* s, Job* j) {
     SCK(cudaMemcpyAsync(s->arena.base + j->prog_off, j->prog.ins.data(), j->prog.ins.size() * sizeof(SrvIns),
                         cudaMemcpyHostToDevice, st));
     SCK(cudaMemcpyAsync(s->arena.base + j->outs_off, j->prog.outs.data(), j->prog.outs.size() * 2, cudaMemcpyHostToDevice, st));
+    s->h2d_bytes += j->prog.ins.size() * sizeof(SrvIns) + j->prog.outs.size() * 2;
     SrvJob& r = j->rec;
     memset(&r, 0, sizeof(r));
     r.prog = (const SrvIns*)(s->arena.base + j->prog_off);
@@ -417,6 +419,8 @@ int run_joins(nsat_server* s, Job* j) {
     memset(h, 0, sizeof(*h));
     for (int i = 0; i < 72; i++) h->best[i] = ~0ull;
     SCK(cudaMemcpyAsync(s->d_join, h, sizeof(*h), cudaMemcpyHostToDevice, st));
+    s->h2d_bytes += sizeof(*h);
+    s->d2h_bytes += sizeof(*h) + 8;
     void* buf[2] = {s->arena.base + j->table_off, s->arena.base + j->table2_off};
     int src = 0;
     for (uint32_t r = 1; r <= j->n; r++) {
@@ -615,6 +619,8 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
     SCK(cudaEventRecord(b.ev1, st));
     b.launched = true;
     s->launches += wide ? 2 : 1;
+    s->h2d_bytes += sizeof(SrvEpoch) + sizeof(SrvJob) * kMaxActive;   // the graph's copies
+    s->d2h_bytes += sizeof(SrvJob) * kMaxActive + kValsCap;
     return NSAT_OK;
 }
 
@@ -744,6 +750,8 @@ extern "C" int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st) {
     st->graph_slots = std::max(s->buf[0].max_slots, s->buf[1].max_slots);
     st->grid = (uint32_t)std::max(s->buf[0].grid, s->buf[1].grid);
     st->launches = s->launches;
+    st->h2d_bytes = s->h2d_bytes;
+    st->d2h_bytes = s->d2h_bytes;
     return NSAT_OK;
 }
 

@@ -90,6 +90,29 @@ __global__ void __launch_bounds__(256) join_round(const typename EntryT<FMT>::ty
     if ((threadIdx.x & 31) == 0 && best != ~0ull) atomicMin(&st->best[r], best);
 }
 
+// Random-gather probe: 8-byte reads from a table of 2^logn entries at
+// addresses spread by a multiplicative hash of the item index (every address
+// is known up front, four loads in flight per thread), folded into one word
+// per thread so no load is dropped.  Its rate is the ceiling of the joins'
+// gathers, which no streaming-copy figure describes.
+__global__ void __launch_bounds__(256) gather_probe(const u64* __restrict__ table, u32 logn, u64 items,
+                                                    u64* __restrict__ out) {
+    const u64 S = (u64)gridDim.x * blockDim.x;
+    const u64 t0 = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    u64 acc = 0;
+    for (u64 i = t0; i < items; i += 4 * S) {
+        u64 v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const u64 j = i + (u64)k * S;
+            const u64 h = (j * 0x9E3779B97F4A7C15ull) >> (64 - logn);
+            v[k] = j < items ? __ldg(table + h) : 0;
+        }
+        acc ^= v[0] ^ v[1] ^ v[2] ^ v[3];
+    }
+    out[t0] = acc;
+}
+
 // LOP3 issue-rate probe: 8 independent chains per thread, each step mixes
 // three previous values so no two steps fold into one LUT.
 template <int LUT>
@@ -146,6 +169,12 @@ extern "C" int nsat_launch_join_round(int fmt, const void* src, void* dst, uint6
     default:
         return -1;
     }
+    return cudaGetLastError() == cudaSuccess ? 0 : -4;
+}
+
+extern "C" int nsat_launch_gather_probe(const uint64_t* table, uint32_t logn, uint64_t items, uint64_t* out,
+                                        int blocks, cudaStream_t stream) {
+    gather_probe<<<blocks, 256, 0, stream>>>((const u64*)table, logn, items, (u64*)out);
     return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 

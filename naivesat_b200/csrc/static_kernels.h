@@ -18,6 +18,10 @@ int nsat_launch_join_round(int fmt, const void* src, void* dst, uint64_t N, uint
                            uint32_t u, uint32_t r, uint32_t mode, NsatJoinState* st,
                            int sm_count, cudaStream_t stream);
 
+// random 8-byte gathers from a table of 2^logn u64 (items reads); out holds
+// blocks * 256 words
+int nsat_launch_gather_probe(const uint64_t* table, uint32_t logn, uint64_t items, uint64_t* out, int blocks,
+                             cudaStream_t stream);
 int nsat_launch_lop3_probe(uint32_t* out, int blocks, int iters, uint64_t* clk,
                            cudaStream_t stream);
 
