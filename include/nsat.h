@@ -302,6 +302,8 @@ typedef struct {
     uint32_t max_slice_tiles;   /* cap of one job's tiles per epoch; 0 = 4096 */
     uint32_t first_slice_tiles; /* a new job's first slice (doubling after); 0 = 1 */
     uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = 1.2e7 */
+    uint32_t build_threads;     /* host threads that build job programs; 0 = min(8, cores / 2) */
+    uint32_t reserved;
 } nsat_server_opts;
 
 typedef struct {
@@ -346,7 +348,12 @@ typedef struct {
 
 int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out);
 void nsat_server_destroy(nsat_server* s);
-/* Queues a job (the circuit is copied); NSAT_EBUSY when the queue is full. */
+/* Queues a job (the circuit is copied) and returns at once: its program is
+ * built on the server's builder threads.  NSAT_EBUSY when the queue is full;
+ * malformed jobs are refused here.  A job whose program cannot be served
+ * (more slots than the interpreter holds: NSAT_EUNSUPPORTED; larger than the
+ * arena: NSAT_ENOMEM) comes back from nsat_server_poll with that status.
+ * submit, step and poll are meant for one caller thread. */
 int nsat_server_submit(nsat_server* s, const nsat_job_desc* job, uint64_t* id);
 /* Admits what fits and runs one epoch; reports jobs still active / queued. */
 int nsat_server_step(nsat_server* s, uint32_t* active, uint32_t* queued);

@@ -104,7 +104,7 @@ class TuneResult(C.Structure):
 class ServerOpts(C.Structure):
     _fields_ = [("arena_bytes", C.c_uint64), ("max_active", C.c_uint32), ("max_queue", C.c_uint32),
                 ("max_slice_tiles", C.c_uint32), ("first_slice_tiles", C.c_uint32),
-                ("epoch_budget", C.c_uint64)]
+                ("epoch_budget", C.c_uint64), ("build_threads", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class JobDesc(C.Structure):
@@ -404,9 +404,10 @@ class Server:
     """Batched serving of many SAT / QSAT / SATOSTOP jobs on one context."""
 
     def __init__(self, ctx, arena_bytes=0, max_active=0, max_queue=0, max_slice_tiles=0,
-                 first_slice_tiles=0, epoch_budget=0):
+                 first_slice_tiles=0, epoch_budget=0, build_threads=0):
         self.ctx = ctx
-        o = ServerOpts(arena_bytes, max_active, max_queue, max_slice_tiles, first_slice_tiles, epoch_budget)
+        o = ServerOpts(arena_bytes, max_active, max_queue, max_slice_tiles, first_slice_tiles, epoch_budget,
+                       build_threads, 0)
         h = C.c_void_p()
         ctx._check(lib().nsat_server_create(ctx.h, C.byref(o), C.byref(h)), "server_create")
         self.h = h
@@ -446,7 +447,8 @@ class Server:
             self.ctx._check(lib().nsat_server_poll(self.h, self._buf, len(self._buf), C.byref(n)), "server_poll")
             for i in range(n.value):
                 r = self._buf[i]
-                d = {"id": r.id, "tag": r.tag, "kind": ["sat", "qsat", "stop"][r.kind], "tiles": r.tiles,
+                d = {"id": r.id, "tag": r.tag, "status": r.status, "kind": ["sat", "qsat", "stop"][r.kind],
+                     "tiles": r.tiles,
                      "submit_ms": r.submit_ms, "admit_ms": r.admit_ms, "done_ms": r.done_ms}
                 if r.kind == 0:
                     d.update(satisfiable=bool(r.satisfiable), count=r.count,

@@ -16,6 +16,10 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <chrono>
 #include <cstring>
 #include <deque>
@@ -223,6 +227,10 @@ struct Job {
     bool any_stop = false;
     bool find_all = false;
     bool finished = false;
+    // program build on a builder thread: 0 pending, 1 built, < 0 status code
+    std::atomic<int> built{0};
+    std::vector<uint32_t> which;     // outputs the program computes
+    std::string build_err;
     uint64_t count = 0;
     nsat_job_result res{};
 };
@@ -265,8 +273,26 @@ struct nsat_server {
     uint64_t epochs = 0, launches = 0;
     uint64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic the server issued
     double device_ms = 0;
+    // builder threads: programs are built off the caller's thread
+    std::mutex bmu;
+    std::condition_variable bcv, built_cv;
+    std::deque<Job*> bqueue;
+    std::vector<std::thread> builders;
+    bool stopping = false;
+
+    void stop_builders() {
+        {
+            std::lock_guard<std::mutex> lk(bmu);
+            stopping = true;
+            bqueue.clear();
+        }
+        bcv.notify_all();
+        for (auto& t : builders) t.join();
+        builders.clear();
+    }
 
     ~nsat_server() {
+        stop_builders();
         cudaSetDevice(ctx_device(ctx));
         cudaStreamSynchronize(ctx_stream(ctx));
         for (EpochBuf& b : buf) {
@@ -447,6 +473,44 @@ int run_joins(nsat_server* s, Job* j) {
 
 }  // namespace
 
+namespace {
+
+// Builder thread: LUT cover, schedule and slot allocation of queued jobs.
+void builder_loop(nsat_server* s, bool raw) {
+    for (;;) {
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->bmu);
+            s->bcv.wait(lk, [s] { return s->stopping || !s->bqueue.empty(); });
+            if (s->stopping) return;
+            j = s->bqueue.front();
+            s->bqueue.pop_front();
+        }
+        std::string err;
+        int st = 1;
+        if (!build_program(j->circ, j->which, raw, &j->prog, &err)) {
+            st = NSAT_EUNSUPPORTED;
+        } else {
+            // a job that could never be admitted is answered with an error
+            // rather than blocking the queue
+            auto round = [](size_t b) { return (b + 255) & ~(size_t)255; };
+            const size_t need = round(prog_bytes(j)) + round(outs_bytes(j)) + 2 * round(table_bytes(j));
+            if (need > s->arena.cap) {
+                st = NSAT_ENOMEM;
+                err = "job needs " + std::to_string(need) + " bytes, the server arena holds " + std::to_string(s->arena.cap);
+            }
+        }
+        j->build_err = err;
+        {
+            std::lock_guard<std::mutex> lk(s->bmu);
+            j->built.store(st, std::memory_order_release);
+        }
+        s->built_cv.notify_all();
+    }
+}
+
+}  // namespace
+
 extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out) {
     if (!ctx || !out) return NSAT_EINVAL;
     *out = nullptr;
@@ -482,6 +546,10 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     SCK(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
     SCK(cudaMalloc(&s->d_join, sizeof(NsatJoinState)));
     SCK(cudaMallocHost(&s->h_join, sizeof(NsatJoinState)));
+    uint32_t nb = s->opts.build_threads;
+    if (!nb) nb = std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
+    const bool raw = ctx_no_optimize(ctx);
+    for (uint32_t t = 0; t < nb; t++) s->builders.emplace_back(builder_loop, s, raw);
     *out = sp.release();
     return NSAT_OK;
 }
@@ -531,16 +599,7 @@ extern "C" int nsat_server_submit(nsat_server* s, const nsat_job_desc* jd, uint6
                 j->qr.reset(new QuantReducer(std::vector<uint8_t>(j->quants.begin(), j->quants.begin() + (j->nb - SRV_TILE_BITS))));
         }
     }
-    std::string err;
-    if (!build_program(j->circ, which, ctx_no_optimize(s->ctx), &j->prog, &err))
-        return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, err);
-    // a job that could never be admitted is refused now rather than blocking the queue
-    auto round = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t need = round(prog_bytes(j.get())) + round(outs_bytes(j.get())) +
-                        2 * round(table_bytes(j.get()));
-    if (need > s->arena.cap)
-        return ctx_fail(s->ctx, NSAT_ENOMEM, "job needs " + std::to_string(need) + " bytes, the server arena holds " +
-                                                 std::to_string(s->arena.cap));
+    j->which = which;
     j->slice = s->opts.first_slice_tiles;
     j->id = s->next_id++;
     j->res.id = j->id;
@@ -548,7 +607,13 @@ extern "C" int nsat_server_submit(nsat_server* s, const nsat_job_desc* jd, uint6
     j->res.kind = j->kind;
     j->res.submit_ms = now_ms();
     *id = j->id;
+    Job* jp = j.get();
     s->queue.push_back(std::move(j));
+    {
+        std::lock_guard<std::mutex> lk(s->bmu);
+        s->bqueue.push_back(jp);
+    }
+    s->bcv.notify_one();
     return NSAT_OK;
 }
 
@@ -693,9 +758,25 @@ int process_epoch(nsat_server* s, EpochBuf& b) {
 extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_queued) {
     if (!s) return NSAT_EINVAL;
     SCK(cudaSetDevice(ctx_device(s->ctx)));
-    // admission in arrival order, by device memory
+    // admission in arrival order, by device memory, of jobs whose program is built
+    if (s->active.empty() && !s->queue.empty()) {
+        // nothing runs: wait (briefly) for the first queued job's program
+        std::unique_lock<std::mutex> lk(s->bmu);
+        Job* f = s->queue.front().get();
+        s->built_cv.wait_for(lk, std::chrono::milliseconds(20),
+                             [f] { return f->built.load(std::memory_order_acquire) != 0; });
+    }
     while (!s->queue.empty() && s->active.size() < s->opts.max_active) {
         Job* j = s->queue.front().get();
+        const int b = j->built.load(std::memory_order_acquire);
+        if (b == 0) break;           // still building
+        if (b < 0) {                 // cannot be served: answered with its status
+            j->res.status = b;
+            j->res.done_ms = now_ms();
+            s->done.push_back(j->res);
+            s->queue.pop_front();
+            continue;
+        }
         int a = admit(s, j);
         if (a < 0) return a;
         if (a > 0) break;   // does not fit yet

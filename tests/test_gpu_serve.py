@@ -109,3 +109,20 @@ def test_admission_by_memory_and_queue_limit(ctx):
     for r in res:
         exp = expected(reqs[r["tag"] % len(reqs)])
         assert project(r, exp) == exp
+
+
+def test_job_larger_than_arena_is_answered_with_enomem(ctx):
+    """Programs are built off the caller's thread; a job that can never fit
+    the arena comes back with NSAT_ENOMEM and the others are served."""
+    reqs = [r for r in small_mix(30, 41) if r["kind"] == "sat"][:6]
+    big = W.random_dag(3, 20, 3000, output="live")
+    srv = api.Server(ctx, arena_bytes=20000, build_threads=2)
+    for i, r in enumerate(reqs):
+        srv.submit("sat", r["circ"], tag=i)
+    srv.submit("sat", big, tag=99)
+    res = {r["tag"]: r for r in srv.run_all()}
+    assert res[99]["status"] == -2
+    for i, r in enumerate(reqs):
+        exp = expected(r)
+        assert res[i]["status"] == 0
+        assert project(res[i], exp) == exp
