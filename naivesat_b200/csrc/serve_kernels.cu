@@ -9,7 +9,7 @@
 // evaluates SRV_WORDS words per program pass, and slot values live in the
 // warp's shared memory laid out [slot][lane][word] (128-bit accesses,
 // conflict-free).  A LUT with a run-time truth table is a 7-lop3 mux tree
-// over the eight truth-table masks of the instruction record.
+// over eight masks expanded from the truth table in the instruction record.
 //
 // Cost per instruction and warp: 3 x 128-bit shared loads, one 128-bit
 // shared store, one uniform 128-bit load of the 16-byte record, 8 byte
