@@ -670,6 +670,8 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
         }
     b.h_hdr->njobs = k;
     b.h_hdr->n_narrow = (uint32_t)sel[0].size();
+    b.h_hdr->hi_mul = 65536;
+    b.h_hdr->slot_bytes = SRV_SLOT_BYTES;
     if (sel[0].empty()) narrow = 16;    // only wide jobs: the narrow launch finds nothing
     cudaGraphExec_t& ge = b.graphs[{narrow, wide}];
     if (!ge) {

@@ -41,7 +41,9 @@ enum { SRV_SAT = 0, SRV_QSAT = 1, SRV_TABLE = 2 };
 struct SrvEpoch {
     uint32_t njobs;
     uint32_t n_narrow;
-    uint32_t pad[62];
+    uint32_t hi_mul;        // 65536 and SRV_SLOT_BYTES, read at run time so the
+    uint32_t slot_bytes;    // kernel's slot decode stays multiply-adds
+    uint32_t pad[60];
 };
 #define SRV_NARROW_SLOTS 48
 

@@ -13,7 +13,9 @@
 //
 // Cost per instruction and warp: 3 x 128-bit shared loads, one 128-bit
 // shared store, one uniform 128-bit load of the 16-byte record, 8 byte
-// permutes that expand the truth table into masks, and 7 * SRV_WORDS lop3.
+// permutes that expand the truth table into masks, 7 * SRV_WORDS lop3, and a
+// slot decode done with multiply-adds so that it runs on the FMA pipe, not on
+// the ALU pipe that bounds the kernel.
 // The L1 data pipe moves 512 bytes per 128-bit warp access, so the record is
 // kept at 16 bytes (a record of eight mask words cost 12 of the
 // instruction's 28 L1 cycles).  Groups of SRV_GROUP independent
@@ -139,11 +141,20 @@ __device__ __forceinline__ u32 lut_mux(u32 a, u32 b, u32 c, const Lut& t) {
     return mux(a, mux(b, x67, x45), mux(b, x23, x01));
 }
 
-__device__ __forceinline__ u32 slot_off(u32 s) { return s * SRV_SLOT_BYTES; }
+// Slot fields decoded with multiply-adds (FMA pipe) instead of masks and
+// shifts (ALU pipe, the kernel's bound): hi = x * km >> 32 with km = 65536,
+// lo = x - hi * km, byte offset = field * sb; km and sb come from the epoch
+// header so they are not folded back into shifts.
+struct Dec { u32 km, sb; };
+__device__ __forceinline__ void fields(u32 x, const Dec& dc, u32* lo, u32* hi) {
+    *hi = __umulhi(x, dc.km);
+    *lo = x - *hi * dc.km;
+}
 
 // Runs a job's program once on this lane's W words.  Sl is the warp's slot
 // area plus lane * W * 4.
-__device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32 ngroups, char* __restrict__ Sl) {
+__device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32 ngroups, char* __restrict__ Sl,
+                                            const Dec& dc) {
     if (ngroups == 0) return;
     const uint4* P = reinterpret_cast<const uint4*>(prog);
     uint4 cur[G];
@@ -151,13 +162,17 @@ __device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32
     for (int k = 0; k < G; k++) cur[k] = __ldg(P + k);
     for (u32 g = 0; g < ngroups; g++) {
         Vals a[G], b[G], c[G];
+        u32 dof[G];
 #pragma unroll
         for (int k = 0; k < G; k++) {
-            a[k] = lds(Sl + slot_off(cur[k].x & 0xffffu));
-            b[k] = lds(Sl + slot_off(cur[k].x >> 16));
-            c[k] = lds(Sl + slot_off(cur[k].y & 0xffffu));
+            u32 al, ah, cl, ch;
+            fields(cur[k].x, dc, &al, &ah);
+            fields(cur[k].y, dc, &cl, &ch);
+            a[k] = lds(Sl + al * dc.sb);
+            b[k] = lds(Sl + ah * dc.sb);
+            c[k] = lds(Sl + cl * dc.sb);
+            dof[k] = ch * dc.sb;
         }
-        // records of the next group (the last group re-reads itself)
         const uint4* nx = P + (size_t)(g + 1 < ngroups ? g + 1 : g) * G;
         uint4 nxt[G];
 #pragma unroll
@@ -168,7 +183,7 @@ __device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32
             Vals d;
 #pragma unroll
             for (int w = 0; w < W; w++) d.v[w] = lut_mux(a[k].v[w], b[k].v[w], c[k].v[w], t);
-            sts(Sl + slot_off(cur[k].y >> 16), d);
+            sts(Sl + dof[k], d);
         }
 #pragma unroll
         for (int k = 0; k < G; k++) cur[k] = nxt[k];
@@ -211,7 +226,8 @@ __device__ __forceinline__ void set_inputs(const SrvJob* J, u64 tile_base, u32 i
 }
 
 // Evaluates tile `tile` of job `J` with this warp.
-__device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ Sl, u32 lane, uint8_t* __restrict__ vals) {
+__device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ Sl, u32 lane, uint8_t* __restrict__ vals,
+                                        const Dec& dc) {
     const u64 tile_base = tile << SRV_TILE_BITS;     // first assignment of the tile
     const u32 kind = J->kind;
     const SrvIns* prog = J->prog;
@@ -224,7 +240,7 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
     const u32 dec_all = J->q0all;
     for (u32 it = 0; it < ITERS; it++) {
         set_inputs(J, tile_base, it, lane, Sl);
-        run_program(prog, ngroups, Sl);
+        run_program(prog, ngroups, Sl, dc);
         if (kind == SRV_SAT) {
             const Vals y = read_out(Sl, J->outs, 0);
 #pragma unroll
@@ -314,6 +330,9 @@ __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict_
     if (cls != 0) jobs += n_narrow;
     const u32 lane = threadIdx.x & 31u;
     char* Sl = smem + lane * (W * 4);
+    Dec dc;
+    dc.km = hdr->hi_mul;
+    dc.sb = hdr->slot_bytes;
     u32 j = njobs ? blockIdx.x % njobs : 0;
     u32 dry = 0;     // consecutive jobs found exhausted
     while (dry < njobs) {
@@ -327,7 +346,7 @@ __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict_
             continue;
         }
         dry = 0;
-        do_tile(J, tile, Sl, lane, vals);
+        do_tile(J, tile, Sl, lane, vals, dc);
     }
 }
 
