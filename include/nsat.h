@@ -301,7 +301,9 @@ typedef struct {
     uint32_t max_queue;         /* waiting jobs before submit returns NSAT_EBUSY; 0 = 2^20 */
     uint32_t max_slice_tiles;   /* cap of one job's tiles per epoch; 0 = 4096 */
     uint32_t first_slice_tiles; /* a new job's first slice (doubling after); 0 = 1 */
-    uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = 1.2e7 */
+    uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = 4.8e7
+                                   (about 30 ms of device time; on the config-4 trace smaller
+                                   budgets raise p99 and lower solves/s) */
     uint32_t build_threads;     /* host threads that build job programs; 0 = min(8, cores / 2) */
     uint32_t reserved;
 } nsat_server_opts;

@@ -523,7 +523,7 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     if (!s->opts.max_queue) s->opts.max_queue = 1u << 20;
     if (!s->opts.max_slice_tiles) s->opts.max_slice_tiles = 4096;
     if (!s->opts.first_slice_tiles) s->opts.first_slice_tiles = 1;
-    if (!s->opts.epoch_budget) s->opts.epoch_budget = 12000000;
+    if (!s->opts.epoch_budget) s->opts.epoch_budget = 48000000;
     SCK(cudaSetDevice(ctx_device(ctx)));
     SCK(cudaMalloc(&s->arena.base, s->opts.arena_bytes));
     s->arena.cap = s->opts.arena_bytes;
