@@ -294,7 +294,9 @@ class StopWorkload:
                "traffic": None, "peak_source": "%s hbm_gbs (MEASURED_PEAKS.json)" % src,
                "kernel": "join_round", "algorithmic_bytes_per_entry_round": 3 * self.eb,
                "rounds": self.rounds, "join_ms": self.join_ms, "build_ms": self.build_ms}
-        out["gather_roofline"] = gather_roofline(self.ctx, self.circ.n, (1 << self.circ.n) * self.rounds,
+        # probe table of the same bytes as this table (u64 probe entries)
+        out["gather_roofline"] = gather_roofline(self.ctx, self.circ.n - (1 if self.eb == 4 else 0),
+                                                 (1 << self.circ.n) * self.rounds,
                                                  (1 << self.circ.n) * self.rounds * 2 * self.eb, self.join_ms, peak)
         return out
 
