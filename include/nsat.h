@@ -216,8 +216,9 @@ int nsat_stop_solve(nsat_ctx* ctx, nsat_table* t, const nsat_stop_opts* opts,
 /* ---- autotuning ----------------------------------------------------------
  * Times the evaluator kernels of one circuit over a sample of its index
  * space with candidate launch shapes -- threads per CTA, CTAs per SM the
- * kernels are compiled for (the register budget), and CTA bits per launch
- * against loop iterations per warp -- and keeps the fastest on the circuit
+ * kernels are compiled for (the register budget), CTA bits per launch
+ * against loop iterations per warp, and the spacing of CTA barriers that keep
+ * a CTA's warps on the same instruction-cache lines -- and keeps the fastest on the circuit
  * handle: later nsat_sat_solve / nsat_qsat_solve calls on that handle use it.
  * Answers are the same under every shape.  Candidates are compiled in
  * parallel host threads.  With persist the choice is reused from / stored in
@@ -236,7 +237,7 @@ typedef struct {
     uint32_t block_threads, min_blocks, cta_bits_max;   /* the chosen shape */
     uint32_t candidates;      /* shapes timed (0 when taken from the cache) */
     uint32_t from_cache;
-    uint32_t reserved;
+    uint32_t sync_every;      /* CTA barrier every this many LUTs in the evaluation (0 = none) */
     double best_rate;         /* assignments per second with the chosen shape */
     double default_rate;      /* ... with the context's shape */
     double tune_ms;           /* wall time of tuning */

@@ -97,7 +97,7 @@ class TuneOpts(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("min_blocks", C.c_uint32), ("cta_bits_max", C.c_uint32),
-                ("candidates", C.c_uint32), ("from_cache", C.c_uint32), ("reserved", C.c_uint32),
+                ("candidates", C.c_uint32), ("from_cache", C.c_uint32), ("sync_every", C.c_uint32),
                 ("best_rate", C.c_double), ("default_rate", C.c_double), ("tune_ms", C.c_double)]
 
 
@@ -367,7 +367,7 @@ class CircuitHandle:
                      q.ctypes.data_as(U8P) if q is not None else None, sample_ms, threads, 0)
         r = TuneResult()
         self.ctx._check(lib().nsat_autotune(self.ctx.h, self.h, C.byref(o), C.byref(r)), "autotune")
-        return {f: getattr(r, f) for f, _ in TuneResult._fields_ if f != "reserved"}
+        return {f: getattr(r, f) for f, _ in TuneResult._fields_}
 
     def autotune_reset(self):
         lib().nsat_autotune_reset(self.h)

@@ -10,7 +10,7 @@ std::string KernelConfig::key() const {
     std::ostringstream s;
     s << "mode=" << (int)mode << " nin=" << nin << " it=" << it << " wb=" << wb << " cb=" << cb
       << " m=" << m << " q0all=" << q0all << " allbits=" << allbits << " data=" << data
-      << " fmt=" << fmt << " nout=" << nout << " minb=" << minb << " map=";
+      << " fmt=" << fmt << " nout=" << nout << " minb=" << minb << " sync=" << sync_every << " map=";
     for (int v : in_of_bit) s << v << ',';
     return s.str();
 }
@@ -30,13 +30,20 @@ __device__ __forceinline__ u32 lop3(u32 a, u32 b, u32 c) {
 
 const uint32_t kLanePat[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
 
-void emit_luts(std::ostringstream& s, const LutNet& net) {
+// sync_every > 0: a CTA barrier after every sync_every LUTs, so the CTA's
+// warps walk the evaluation code together and share instruction-cache lines
+// (the unrolled evaluation of a large circuit is larger than the
+// instruction cache; c1 at 64: ALU pipe 89 % -> 0.99 of the lop3 peak).  Only
+// for kernels whose every thread runs the same number of evaluations.
+void emit_luts(std::ostringstream& s, const LutNet& net, uint32_t sync_every = 0) {
     for (uint32_t i : net.used_inputs) s << "    const u32 w" << i << " = x[" << i << "];\n";
     char buf[160];
+    uint32_t k = 0;
     for (const Lut& L : net.luts) {
         snprintf(buf, sizeof(buf), "    const u32 w%u = lop3<0x%02x>(w%u, w%u, w%u);\n", L.wire,
                  L.tt, L.in[0], L.in[1], L.in[2]);
         s << buf;
+        if (sync_every && ++k % sync_every == 0) s << "    __syncthreads();\n";
     }
 }
 
@@ -110,7 +117,10 @@ std::string generate_source(const KernelConfig& kc, const LutNet& net) {
     } else {
         s << "__device__ __forceinline__ u32 nsat_eval1(const u32* x) {\n";
         if (!kc.data) {
-            emit_luts(s, net);
+            // the SAT and QSAT kernels run the same number of evaluations in
+            // every thread of a CTA, so barriers inside the evaluation are safe
+            const bool uniform = kc.mode == Mode::SAT || kc.mode == Mode::QSAT;
+            emit_luts(s, net, uniform && kc.threads() > 32 ? kc.sync_every : 0);
             s << "    return " << (net.outs[0].neg ? "~" : "") << "w" << net.outs[0].wire << ";\n";
         } else {
             s << "    return 0u;\n";

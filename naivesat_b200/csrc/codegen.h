@@ -17,6 +17,7 @@ struct KernelConfig {
     std::vector<int> in_of_bit;  // enumeration bit -> circuit input
     uint32_t it = 0, wb = 0, cb = 0;  // log2 iterations/warp, warps/CTA, CTAs/launch
     uint32_t minb = 0;         // __launch_bounds__ minimum CTAs per SM (0 = none)
+    uint32_t sync_every = 0;   // SAT/QSAT: CTA barrier after every this many LUTs (0 = none)
     uint32_t c = 0;            // 10 + it + wb + cb
     // QSAT
     uint32_t m = 0;            // unit level (inner bits below the first block)

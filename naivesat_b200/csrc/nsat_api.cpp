@@ -72,7 +72,13 @@ struct nsat_ctx {
 // a launch's bits are loop iterations per warp).  0 = the context's choice.
 struct Shape {
     uint32_t block_threads = 0, min_blocks = 0, cb_max = 0;
+    uint32_t sync_every = 0;     // 0 = default (kDefaultSync); kNoSync = no barriers
 };
+
+constexpr uint32_t kDefaultSync = 64;
+constexpr uint32_t kNoSync = 0xffffffffu;
+
+uint32_t sync_of(const Shape& sh) { return sh.sync_every == kNoSync ? 0 : (sh.sync_every ? sh.sync_every : kDefaultSync); }
 
 struct nsat_circuit {
     nsat_ctx* ctx = nullptr;
@@ -153,6 +159,7 @@ Shape effective_shape(const nsat_ctx* ctx, const Shape& tuned) {
     s.block_threads = tuned.block_threads ? tuned.block_threads : ctx->opts.block_threads;
     s.min_blocks = tuned.block_threads ? tuned.min_blocks : ctx->opts.min_blocks;
     s.cb_max = tuned.cb_max;
+    s.sync_every = tuned.sync_every;
     return s;
 }
 
@@ -302,6 +309,7 @@ int plan_sat(uint32_t n, const nsat_sat_opts& o, const Shape& sh, SatPlan* pl, s
     for (uint32_t p = 0; p < np; p++) kc.in_of_bit[p] = p < d ? -1 : (int)(p - d);
     choose_shape(C, block_threads, &kc, sh.cb_max);
     kc.minb = min_blocks ? min_blocks : default_min_blocks(kc);
+    kc.sync_every = sync_of(sh);
     pl->d = d; pl->C = C; pl->bp = bp; pl->ep = ep;
     return NSAT_OK;
 }
@@ -347,6 +355,7 @@ int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint
     }
     choose_shape(C, block_threads, &kc, sh.cb_max);
     kc.minb = min_blocks ? min_blocks : default_min_blocks(kc);
+    kc.sync_every = sync_of(sh);
     kc.m = std::min<uint32_t>(m, 127);
     kc.q0all = q[s] != 0;
     kc.allbits = 0;
@@ -1193,7 +1202,7 @@ void precompile(nsat_ctx* ctx, nsat_circuit* c, uint32_t kind, const std::vector
 }
 
 std::string tune_key(nsat_ctx* ctx, nsat_circuit* c, uint32_t kind, const uint8_t* quants) {
-    std::string k = "tune1|" + std::to_string(kind) + "|" + std::to_string(c->circ.n) + "|";
+    std::string k = "tune2|" + std::to_string(kind) + "|" + std::to_string(c->circ.n) + "|";
     for (const Gate& g : c->circ.gates) k += std::to_string(g.func) + "," + std::to_string(g.i0) + "," + std::to_string(g.i1) + ";";
     k += "|";
     for (const Output& o : c->circ.outputs) k += std::to_string(o.wire) + (o.neg ? "n;" : ";");
@@ -1228,13 +1237,14 @@ extern "C" int nsat_autotune(nsat_ctx* ctx, nsat_circuit* c, const nsat_tune_opt
     if (opts->persist) {
         FILE* f = fopen(path.c_str(), "r");
         if (f) {
-            unsigned bt = 0, mb = 0, cb = 0;
+            unsigned bt = 0, mb = 0, cb = 0, sy = 0;
             double rate = 0, drate = 0;
-            const int got = fscanf(f, "%u %u %u %lf %lf", &bt, &mb, &cb, &rate, &drate);
+            const int got = fscanf(f, "%u %u %u %u %lf %lf", &bt, &mb, &cb, &sy, &rate, &drate);
             fclose(f);
-            if (got == 5 && bt) {
-                slot.block_threads = bt; slot.min_blocks = mb; slot.cb_max = cb;
+            if (got == 6 && bt) {
+                slot.block_threads = bt; slot.min_blocks = mb; slot.cb_max = cb; slot.sync_every = sy;
                 res->block_threads = bt; res->min_blocks = mb; res->cta_bits_max = cb;
+                res->sync_every = sync_of(slot);
                 res->best_rate = rate; res->default_rate = drate;
                 res->from_cache = 1;
                 res->tune_ms = now_ms() - t0;
@@ -1279,6 +1289,19 @@ extern "C" int nsat_autotune(nsat_ctx* ctx, nsat_circuit* c, const nsat_tune_opt
         res->candidates++;
         if (cd.rate > best.rate * 1.01) best = cd;     // keep the default CTA cap unless clearly faster
     }
+    // stage 3: CTA barrier spacing in the evaluation (instruction-cache sharing)
+    std::vector<Candidate> st3;
+    for (uint32_t sy : {kNoSync, 32u, 128u}) {
+        Candidate cd = best;
+        cd.sh.sync_every = sy;
+        st3.push_back(cd);
+    }
+    precompile(ctx, c, kind, q, st3, opts->threads);
+    for (Candidate& cd : st3) {
+        if (int rc = measure_shape(ctx, c, kind, opts->quants, cd.sh, sample, &cd.rate)) return rc;
+        res->candidates++;
+        if (cd.rate > best.rate * 1.01) best = cd;
+    }
     // the winner and the default once more, back to back
     double again = 0, def_again = 0;
     if (int rc = measure_shape(ctx, c, kind, opts->quants, best.sh, sample, &again)) return rc;
@@ -1295,14 +1318,15 @@ extern "C" int nsat_autotune(nsat_ctx* ctx, nsat_circuit* c, const nsat_tune_opt
     res->block_threads = slot.block_threads;
     res->min_blocks = slot.min_blocks;
     res->cta_bits_max = slot.cb_max;
+    res->sync_every = sync_of(slot);
     res->best_rate = best.rate;
     res->default_rate = default_rate;
     if (opts->persist) {
         const std::string tmp = path + ".tmp";
         FILE* f = fopen(tmp.c_str(), "w");
         if (f) {
-            fprintf(f, "%u %u %u %.6e %.6e\n", slot.block_threads, slot.min_blocks, slot.cb_max, best.rate,
-                    default_rate);
+            fprintf(f, "%u %u %u %u %.6e %.6e\n", slot.block_threads, slot.min_blocks, slot.cb_max,
+                    slot.sync_every, best.rate, default_rate);
             fclose(f);
             rename(tmp.c_str(), path.c_str());
         }
