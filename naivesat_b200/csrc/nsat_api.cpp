@@ -182,9 +182,13 @@ void choose_shape(uint32_t C, uint32_t block_threads, KernelConfig* kc, uint32_t
 // not say: 24 warps per SM (80 registers per thread, no spills on the
 // 3000-gate circuits) measured 9 % faster than the register-unbounded
 // 16-warp build on c1; tiny kernels are not register limited either way.
-uint32_t default_min_blocks(const KernelConfig& kc) {
+// Circuits of at most 64 mapped lop3 (e.g. the 32-input adder QSAT) are
+// bound by the reduction stages' latency, not by registers: 48 warps per SM
+// measured 18 % faster than 24 there and no better elsewhere.
+uint32_t default_min_blocks(const KernelConfig& kc, uint32_t lop3) {
     const uint32_t warps = 1u << kc.wb;
-    return warps >= 24 ? 1 : 24 / warps;
+    const uint32_t target = (lop3 && lop3 <= 64) ? 48 : 24;
+    return warps >= target ? 1 : target / warps;
 }
 
 int ensure_scratch(nsat_ctx* ctx, size_t bytes) {
@@ -284,7 +288,7 @@ struct SatPlan {
     u128 bp = 0, ep = 0;   // range in the padded index space
 };
 
-int plan_sat(uint32_t n, const nsat_sat_opts& o, const Shape& sh, SatPlan* pl, std::string* err) {
+int plan_sat(uint32_t n, const nsat_sat_opts& o, const Shape& sh, SatPlan* pl, std::string* err, uint32_t lop3 = 0) {
     const uint32_t block_threads = sh.block_threads, min_blocks = sh.min_blocks;
     const uint32_t d = n < 15 ? 15 - n : 0;     // dummy low bits for tiny circuits
     const uint32_t np = n + d;
@@ -308,7 +312,7 @@ int plan_sat(uint32_t n, const nsat_sat_opts& o, const Shape& sh, SatPlan* pl, s
     kc.in_of_bit.resize(np);
     for (uint32_t p = 0; p < np; p++) kc.in_of_bit[p] = p < d ? -1 : (int)(p - d);
     choose_shape(C, block_threads, &kc, sh.cb_max);
-    kc.minb = min_blocks ? min_blocks : default_min_blocks(kc);
+    kc.minb = min_blocks ? min_blocks : default_min_blocks(kc, lop3);
     kc.sync_every = sync_of(sh);
     pl->d = d; pl->C = C; pl->bp = bp; pl->ep = ep;
     return NSAT_OK;
@@ -324,7 +328,7 @@ struct QsatPlan {
 };
 
 int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint32_t chunk_bits,
-              const Shape& sh, uint32_t prefix_bits, QsatPlan* pl, std::string* err) {
+              const Shape& sh, uint32_t prefix_bits, QsatPlan* pl, std::string* err, uint32_t lop3 = 0) {
     const uint32_t block_threads = sh.block_threads, min_blocks = sh.min_blocks;
     if (quants_in.size() != n || n == 0) { *err = "quantifier count differs from inputs"; return NSAT_EINVAL; }
     if (prefix_bits >= n) { *err = "prefix must leave at least one free input"; return NSAT_EINVAL; }
@@ -354,7 +358,7 @@ int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint
         kc.in_of_bit[p] = (data || in >= (int)n) ? -1 : in;
     }
     choose_shape(C, block_threads, &kc, sh.cb_max);
-    kc.minb = min_blocks ? min_blocks : default_min_blocks(kc);
+    kc.minb = min_blocks ? min_blocks : default_min_blocks(kc, lop3);
     kc.sync_every = sync_of(sh);
     kc.m = std::min<uint32_t>(m, 127);
     kc.q0all = q[s] != 0;
@@ -561,12 +565,13 @@ extern "C" int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opt
     if (opts) o = *opts;
     SatPlan plan;
     std::string perr;
-    if (int rc = plan_sat(c->circ.n, o, effective_shape(ctx, c->tuned), &plan, &perr)) return fail(ctx, rc, perr);
+    const std::vector<uint32_t> out0{0};
+    const LutNet& net = get_net(c, out0);
+    if (int rc = plan_sat(c->circ.n, o, effective_shape(ctx, c->tuned), &plan, &perr, (uint32_t)net.luts.size()))
+        return fail(ctx, rc, perr);
     const KernelConfig& kc = plan.kc;
     const uint32_t d = plan.d, C = plan.C;
     const u128 bp = plan.bp, ep = plan.ep;
-    const std::vector<uint32_t> out0{0};
-    const LutNet& net = get_net(c, out0);
     CUfunction fn;
     std::shared_ptr<JitModule> mod;
     if (int rc = get_kernel(ctx, kc, net, "nsat_sat", &fn, &mod)) return rc;
@@ -632,8 +637,12 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     const uint32_t n = data ? n_items_bits : c->circ.n;
     QsatPlan plan;
     std::string perr;
+    LutNet empty;
+    const std::vector<uint32_t> out0{0};
+    const LutNet& net = data ? empty : get_net(c, out0);
     const Shape sh = data ? effective_shape(ctx, Shape()) : effective_shape(ctx, c->tuned_qsat);
-    if (int rc = plan_qsat(n, quants_in, data, chunk_bits, sh, prefix_bits, &plan, &perr))
+    if (int rc = plan_qsat(n, quants_in, data, chunk_bits, sh, prefix_bits, &plan, &perr,
+                           data ? 0u : (uint32_t)net.luts.size()))
         return fail(ctx, rc, perr);
     if (prefix_bits < 64 && (prefix >> prefix_bits) != 0) return fail(ctx, NSAT_EINVAL, "prefix wider than prefix_bits");
     const KernelConfig& kc = plan.kc;
@@ -644,9 +653,6 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     const uint32_t d = plan.d, np = plan.np, m = plan.m, C = plan.C, s = plan.s, f = plan.fsub;
     const uint32_t A = plan.A - s;
     const uint64_t L0 = s ? (prefix << A) : 0;
-    LutNet empty;
-    const std::vector<uint32_t> out0{0};
-    const LutNet& net = data ? empty : get_net(c, out0);
     CUfunction fn;
     std::shared_ptr<JitModule> mod;
     if (int rc = get_kernel(ctx, kc, net, "nsat_qsat", &fn, &mod)) return rc;
@@ -1050,28 +1056,30 @@ extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quan
     sh.min_blocks = opts ? opts->min_blocks : 0;
     KernelConfig kc;
     std::vector<uint32_t> which{0};
+    if (kind == 2) {
+        which.clear();
+        for (uint32_t j = 0; j < c.outputs.size(); j++) which.push_back(j);
+    }
+    LutNet net = map_luts(c, which, raw);
     std::string err;
     int rc;
     if (kind == 0) {
         SatPlan pl;
         nsat_sat_opts so{};
         so.find_all = 1;
-        rc = plan_sat(c.n, so, sh, &pl, &err);
+        rc = plan_sat(c.n, so, sh, &pl, &err, (uint32_t)net.luts.size());
         kc = pl.kc;
     } else if (kind == 1) {
         if (!quants) return NSAT_EINVAL;
         std::vector<uint8_t> q(quants, quants + c.n);
         for (auto& v : q) v = v ? 1 : 0;
         QsatPlan pl;
-        rc = plan_qsat(c.n, q, false, 0, sh, 0, &pl, &err);
+        rc = plan_qsat(c.n, q, false, 0, sh, 0, &pl, &err, (uint32_t)net.luts.size());
         kc = pl.kc;
     } else {
         rc = plan_table(c, false, &kc, &err);
-        which.clear();
-        for (uint32_t j = 0; j < c.outputs.size(); j++) which.push_back(j);
     }
     if (rc) return rc;
-    LutNet net = map_luts(c, which, raw);
     info->lop3_ops = (uint32_t)net.luts.size();
     info->live_gates = net.live_gates;
     std::string src = generate_source(kc, net);
@@ -1172,11 +1180,11 @@ void precompile(nsat_ctx* ctx, nsat_circuit* c, uint32_t kind, const std::vector
             SatPlan pl;
             nsat_sat_opts o{};
             o.find_all = 1;
-            if (plan_sat(c->circ.n, o, sh, &pl, &err)) continue;
+            if (plan_sat(c->circ.n, o, sh, &pl, &err, (uint32_t)net.luts.size())) continue;
             kc = pl.kc;
         } else {
             QsatPlan pl;
-            if (plan_qsat(c->circ.n, q, false, 0, sh, 0, &pl, &err)) continue;
+            if (plan_qsat(c->circ.n, q, false, 0, sh, 0, &pl, &err, (uint32_t)net.luts.size())) continue;
             kc = pl.kc;
         }
         srcs.push_back(generate_source(kc, net));
