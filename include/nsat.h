@@ -306,7 +306,15 @@ typedef struct {
                                    (about 30 ms of device time; on the config-4 trace smaller
                                    budgets raise p99 and lower solves/s) */
     uint32_t build_threads;     /* host threads that build job programs; 0 = min(8, cores / 2) */
-    uint32_t reserved;
+    uint32_t tier_threads;      /* QSAT tiering workers (own context each); 0 = half the host
+                                   threads, between 2 and 12 */
+    uint32_t tier_min_ms;       /* QSAT jobs whose whole index space would take the interpreter
+                                   longer than this (estimate) race a compiled kernel: it is
+                                   compiled in the background and, once ready, solves the job's
+                                   remaining 1/16 blocks as prefix sub-problems; 0 = 30,
+                                   0xFFFFFFFF = never */
+    uint32_t tier_wait;         /* 1: such a job is not interpreted until its kernel is ready, so
+                                   every block runs compiled (compile first instead of racing) */
 } nsat_server_opts;
 
 typedef struct {
@@ -335,8 +343,10 @@ typedef struct {
     int32_t found;              /* SATOSTOP */
     uint64_t solution;
     uint64_t start, end, steps; /* SATOSTOP */
-    uint64_t tiles;             /* tiles evaluated */
+    uint64_t tiles;             /* tiles evaluated by the interpreter */
     double submit_ms, admit_ms, done_ms;   /* steady clock, milliseconds */
+    uint32_t compiled_blocks;   /* QSAT: prefix blocks solved by a compiled kernel (tiering) */
+    uint32_t reserved;
 } nsat_job_result;
 
 typedef struct {

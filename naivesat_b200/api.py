@@ -104,7 +104,8 @@ class TuneResult(C.Structure):
 class ServerOpts(C.Structure):
     _fields_ = [("arena_bytes", C.c_uint64), ("max_active", C.c_uint32), ("max_queue", C.c_uint32),
                 ("max_slice_tiles", C.c_uint32), ("first_slice_tiles", C.c_uint32),
-                ("epoch_budget", C.c_uint64), ("build_threads", C.c_uint32), ("reserved", C.c_uint32)]
+                ("epoch_budget", C.c_uint64), ("build_threads", C.c_uint32), ("tier_threads", C.c_uint32),
+                ("tier_min_ms", C.c_uint32), ("tier_wait", C.c_uint32)]
 
 
 class JobDesc(C.Structure):
@@ -120,7 +121,7 @@ class JobResult(C.Structure):
                 ("solution_bits", C.c_uint32), ("has_solution", C.c_int32), ("found", C.c_int32),
                 ("solution", C.c_uint64), ("start", C.c_uint64), ("end", C.c_uint64), ("steps", C.c_uint64),
                 ("tiles", C.c_uint64), ("submit_ms", C.c_double), ("admit_ms", C.c_double),
-                ("done_ms", C.c_double)]
+                ("done_ms", C.c_double), ("compiled_blocks", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
@@ -404,10 +405,11 @@ class Server:
     """Batched serving of many SAT / QSAT / SATOSTOP jobs on one context."""
 
     def __init__(self, ctx, arena_bytes=0, max_active=0, max_queue=0, max_slice_tiles=0,
-                 first_slice_tiles=0, epoch_budget=0, build_threads=0):
+                 first_slice_tiles=0, epoch_budget=0, build_threads=0, tier_threads=0, tier_min_ms=0,
+                 tier_wait=False):
         self.ctx = ctx
         o = ServerOpts(arena_bytes, max_active, max_queue, max_slice_tiles, first_slice_tiles, epoch_budget,
-                       build_threads, 0)
+                       build_threads, tier_threads, tier_min_ms, 1 if tier_wait else 0)
         h = C.c_void_p()
         ctx._check(lib().nsat_server_create(ctx.h, C.byref(o), C.byref(h)), "server_create")
         self.h = h
@@ -448,7 +450,7 @@ class Server:
             for i in range(n.value):
                 r = self._buf[i]
                 d = {"id": r.id, "tag": r.tag, "status": r.status, "kind": ["sat", "qsat", "stop"][r.kind],
-                     "tiles": r.tiles,
+                     "tiles": r.tiles, "compiled_blocks": r.compiled_blocks,
                      "submit_ms": r.submit_ms, "admit_ms": r.admit_ms, "done_ms": r.done_ms}
                 if r.kind == 0:
                     d.update(satisfiable=bool(r.satisfiable), count=r.count,

@@ -18,6 +18,8 @@ int ctx_device(const nsat_ctx* ctx);
 cudaStream_t ctx_stream(const nsat_ctx* ctx);
 int ctx_sm_count(const nsat_ctx* ctx);
 bool ctx_no_optimize(const nsat_ctx* ctx);
+// The options a context was created with.
+nsat_opts ctx_opts(const nsat_ctx* ctx);
 // Records a failure on the context (nsat_last_error) and returns `code`.
 int ctx_fail(nsat_ctx* ctx, int code, const std::string& msg);
 

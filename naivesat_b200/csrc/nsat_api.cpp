@@ -767,6 +767,7 @@ int nsat::ctx_device(const nsat_ctx* ctx) { return ctx ? ctx->device : -1; }
 cudaStream_t nsat::ctx_stream(const nsat_ctx* ctx) { return ctx->stream; }
 int nsat::ctx_sm_count(const nsat_ctx* ctx) { return ctx->sm_count; }
 bool nsat::ctx_no_optimize(const nsat_ctx* ctx) { return ctx->opts.no_optimize != 0; }
+nsat_opts nsat::ctx_opts(const nsat_ctx* ctx) { return ctx->opts; }
 int nsat::ctx_fail(nsat_ctx* ctx, int code, const std::string& msg) { return fail(ctx, code, msg); }
 Circuit nsat::circuit_from_desc(const nsat_circuit_desc* d) { return from_desc(d); }
 

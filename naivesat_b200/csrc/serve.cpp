@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <array>
+#include <cmath>
 #include <atomic>
 #include <condition_variable>
 #include <mutex>
@@ -44,6 +45,7 @@ namespace {
 
 constexpr uint32_t kMaxActive = 512;
 constexpr size_t kValsCap = 256 * 1024;      // QSAT tile values per epoch
+constexpr double kInterpRate = 1.5e12;        // interpreter LUT-words/s (measured), for the tiering estimate
 
 double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -233,7 +235,22 @@ struct Job {
     std::string build_err;
     uint64_t count = 0;
     nsat_job_result res{};
+    // QSAT tiering: a compiled kernel races the interpreter (see tier_loop)
+    std::atomic<int> tier{0};            // TIER_* below
+    std::atomic<bool> tier_cancel{false};
+    std::atomic<int64_t> run_from{-1};   // first block the worker solves (set by step)
+    uint32_t tier_s = 0;                 // prefix bits of a block
+    uint64_t tier_block = 0;             // tiles per block
+    uint64_t stop_at = UINT64_MAX;       // the interpreter stops at this tile
+    uint64_t next_block = 0;             // next block result to fold in
+    std::mutex tmu;                      // guards blk
+    std::condition_variable tcv;         // run_from / cancel for the worker
+    std::map<uint64_t, nsat_qsat_result> blk;   // block results by prefix
+    int tier_rc = NSAT_OK;
+    bool emitted = false;                // result handed to poll, arena memory released
 };
+
+enum { TIER_NONE = 0, TIER_COMPILING = 1, TIER_READY = 2, TIER_RUNNING = 3, TIER_DONE = 4 };
 
 // One of the two epoch buffers: while the device runs the epoch of one, the
 // host reads the results of the other and fills it again.
@@ -261,6 +278,7 @@ struct nsat_server {
     Arena arena;
     std::deque<std::unique_ptr<Job>> queue;
     std::vector<std::unique_ptr<Job>> active;
+    std::vector<std::unique_ptr<Job>> parked;   // answered jobs a tiering worker still reads
     std::vector<nsat_job_result> done;
     uint64_t next_id = 1;
     uint32_t rr = 0;   // rotating start of the epoch table
@@ -279,6 +297,25 @@ struct nsat_server {
     std::deque<Job*> bqueue;
     std::vector<std::thread> builders;
     bool stopping = false;
+    // QSAT tiering workers, each with its own context on the device
+    std::mutex tqmu;
+    std::condition_variable tqcv;
+    std::deque<Job*> tqueue;
+    std::vector<std::thread> tier_workers;
+    std::atomic<bool> tstop{false};
+    bool tier_enabled = false;
+
+    void stop_tiers() {
+        tstop = true;
+        {
+            std::lock_guard<std::mutex> lk(tqmu);
+            for (Job* j : tqueue) j->tier = TIER_DONE;
+            tqueue.clear();
+        }
+        tqcv.notify_all();
+        for (auto& t : tier_workers) t.join();
+        tier_workers.clear();
+    }
 
     void stop_builders() {
         {
@@ -293,6 +330,7 @@ struct nsat_server {
 
     ~nsat_server() {
         stop_builders();
+        stop_tiers();
         cudaSetDevice(ctx_device(ctx));
         cudaStreamSynchronize(ctx_stream(ctx));
         for (EpochBuf& b : buf) {
@@ -501,12 +539,106 @@ void builder_loop(nsat_server* s, bool raw) {
             }
         }
         j->build_err = err;
+        // QSAT jobs that would keep the interpreter busy long race a compiled kernel
+        if (st == 1 && j->kind == SRV_QSAT && j->d == 0 && j->nb >= SRV_TILE_BITS + 4 && j->nb <= 60 &&
+            s->tier_enabled) {
+            const double est_ms = std::ldexp(1.0, (int)j->nb - 5) * (double)j->prog.ins.size() / kInterpRate * 1e3;
+            if (est_ms > (double)s->opts.tier_min_ms) {
+                j->tier_s = 4;
+                j->tier_block = j->total_tiles >> j->tier_s;
+                j->tier = TIER_COMPILING;
+                {
+                    std::lock_guard<std::mutex> lk(s->tqmu);
+                    s->tqueue.push_back(j);
+                }
+                s->tqcv.notify_one();
+            }
+        }
         {
             std::lock_guard<std::mutex> lk(s->bmu);
             j->built.store(st, std::memory_order_release);
         }
         s->built_cv.notify_all();
     }
+}
+
+// Tiering worker: compiles a QSAT job's kernel for sub-problems under a
+// tier_s-input prefix (a warm solve of the last block, whose result is kept),
+// reports ready, waits until the server has stopped interpreting at a block
+// boundary, then solves the remaining blocks in order, posting each result.
+// Blocks are solved by the one-shot QSAT solver on the worker's own context
+// and stream, concurrently with the interpreter epochs.
+void tier_loop(nsat_server* s, nsat_opts copts) {
+    nsat_ctx* wctx = nullptr;
+    if (nsat_create(ctx_device(s->ctx), &copts, &wctx) != NSAT_OK) wctx = nullptr;
+    for (;;) {
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->tqmu);
+            s->tqcv.wait(lk, [s] { return s->tstop.load() || !s->tqueue.empty(); });
+            if (s->tstop) break;
+            j = s->tqueue.front();
+            s->tqueue.pop_front();
+        }
+        if (!wctx || j->tier_cancel) {
+            j->tier = TIER_DONE;
+            continue;
+        }
+        const uint32_t sbits = j->tier_s;
+        const uint64_t nblocks = 1ull << sbits;
+        // the circuit on this worker's context
+        std::vector<uint32_t> gates, outs;
+        for (const Gate& g : j->circ.gates) { gates.push_back(g.func); gates.push_back(g.i0); gates.push_back(g.i1); }
+        for (const Output& o : j->circ.outputs) { outs.push_back(o.wire); outs.push_back(o.neg ? 1 : 0); }
+        nsat_circuit_desc desc{j->circ.n, (uint32_t)j->circ.gates.size(), gates.data(),
+                               (uint32_t)j->circ.outputs.size(), outs.data()};
+        nsat_circuit* cw = nullptr;
+        int rc = nsat_circuit_new(wctx, &desc, &cw);
+        auto solve = [&](uint64_t p, nsat_qsat_result* r) {
+            nsat_qsat_opts qo{};
+            qo.prefix_bits = sbits;
+            qo.prefix = p;
+            return nsat_qsat_solve(wctx, cw, j->quants.data(), &qo, r);
+        };
+        if (rc == NSAT_OK) {
+            nsat_qsat_result r{};
+            rc = solve(nblocks - 1, &r);   // compiles and loads the kernel
+            if (rc == NSAT_OK) {
+                std::lock_guard<std::mutex> lk(j->tmu);
+                j->blk[nblocks - 1] = r;
+            }
+        }
+        if (rc != NSAT_OK) {
+            j->tier_rc = rc;
+            if (cw) nsat_circuit_free(cw);
+            j->tier = TIER_DONE;
+            continue;
+        }
+        j->tier = TIER_READY;
+        // wait for the handoff (or a cancel)
+        int64_t from = -1;
+        {
+            std::unique_lock<std::mutex> lk(j->tmu);
+            while (!j->tier_cancel && !s->tstop && (from = j->run_from.load()) < 0)
+                j->tcv.wait_for(lk, std::chrono::milliseconds(50));
+        }
+        if (from >= 0 && !j->tier_cancel && !s->tstop) {
+            j->tier = TIER_RUNNING;
+            for (uint64_t p = (uint64_t)from; p + 1 < nblocks; p++) {
+                if (j->tier_cancel || s->tstop) break;
+                nsat_qsat_result r{};
+                if (solve(p, &r) != NSAT_OK) {
+                    j->tier_rc = NSAT_ECUDA;
+                    break;
+                }
+                std::lock_guard<std::mutex> lk(j->tmu);
+                j->blk[p] = r;
+            }
+        }
+        nsat_circuit_free(cw);
+        j->tier = TIER_DONE;
+    }
+    if (wctx) nsat_destroy(wctx);
 }
 
 }  // namespace
@@ -546,10 +678,18 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     SCK(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
     SCK(cudaMalloc(&s->d_join, sizeof(NsatJoinState)));
     SCK(cudaMallocHost(&s->h_join, sizeof(NsatJoinState)));
+    // defaults measured on the config-4 trace (3000 requests): 30 ms and 8
+    // workers took 366 -> 609 solves/s and p99 at 150/s 172 -> 42 ms
+    if (s->opts.tier_min_ms == 0) s->opts.tier_min_ms = 30;
+    const uint32_t hw_tier = std::max(2u, std::min(12u, std::thread::hardware_concurrency() / 2));
+    const uint32_t ntier =
+        s->opts.tier_min_ms == 0xffffffffu ? 0 : (s->opts.tier_threads ? s->opts.tier_threads : hw_tier);
+    s->tier_enabled = ntier > 0;
     uint32_t nb = s->opts.build_threads;
     if (!nb) nb = std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
     const bool raw = ctx_no_optimize(ctx);
     for (uint32_t t = 0; t < nb; t++) s->builders.emplace_back(builder_loop, s, raw);
+    for (uint32_t t = 0; t < ntier; t++) s->tier_workers.emplace_back(tier_loop, s, ctx_opts(ctx));
     *out = sp.release();
     return NSAT_OK;
 }
@@ -632,7 +772,10 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
     for (uint32_t t = 0; t < na; t++) {
         Job* j = s->active[(s->rr + t) % na].get();
         if (j->finished) continue;
-        uint64_t want = std::min<uint64_t>(j->slice, j->total_tiles - j->sched);
+        if (s->opts.tier_wait && j->tier.load() == TIER_COMPILING) continue;   // compile first
+        const uint64_t lim = std::min<uint64_t>(j->total_tiles, j->stop_at);
+        if (j->sched >= lim) continue;
+        uint64_t want = std::min<uint64_t>(j->slice, lim - j->sched);
         const uint64_t cost_per_tile = std::max<uint64_t>(1, j->prog.ins.size());
         if (k > 0 && want * cost_per_tile > budget) want = budget / cost_per_tile;
         if (j->kind == SRV_QSAT && j->qr) want = std::min<uint64_t>(want, kValsCap - vals);
@@ -755,6 +898,77 @@ int process_epoch(nsat_server* s, EpochBuf& b) {
     return NSAT_OK;
 }
 
+// The QSAT tiering protocol on the server's side, once per step: when a
+// job's compiled kernel is ready, the interpreter stops at the next block
+// boundary; once every interpreted tile below it is folded in, the worker
+// gets the remaining blocks; their results are folded in block order.  A
+// block that holds whole first-block units ends the job when it has a
+// decisive unit (its witness completes the prefix); otherwise, and for a
+// block inside one unit, the block's value stands for each of its tiles in
+// the job's forall/exists reducer (the reduction of equal values is that
+// value).
+void tier_step(nsat_server* s, Job* j) {
+    const int t = j->tier.load();
+    if (t == TIER_NONE || j->finished) return;
+    const uint64_t B = j->tier_block, nblocks = 1ull << j->tier_s;
+    if (t >= TIER_READY && j->stop_at == UINT64_MAX && j->tier_rc == NSAT_OK)
+        j->stop_at = (j->sched + B - 1) / B * B;
+    if (j->stop_at != UINT64_MAX && j->run_from.load() < 0 && j->cursor == j->stop_at && j->inflight == 0) {
+        if (j->stop_at >= j->total_tiles) {
+            j->tier_cancel = true;       // the interpreter covered every tile
+        } else {
+            {
+                std::lock_guard<std::mutex> lk(j->tmu);
+                j->run_from = (int64_t)(j->stop_at / B);
+                j->next_block = j->stop_at / B;
+            }
+            j->tcv.notify_all();
+        }
+    }
+    if (j->run_from.load() < 0) return;
+    for (;;) {
+        nsat_qsat_result r{};
+        {
+            std::lock_guard<std::mutex> lk(j->tmu);
+            auto it = j->blk.find(j->next_block);
+            if (it == j->blk.end()) break;
+            r = it->second;
+        }
+        const uint64_t p = j->next_block++;
+        j->res.compiled_blocks++;
+        bool finished = false;
+        if (j->tier_s < j->f && r.has_solution) {
+            // decisive unit in this block: prefix bits, then the block's own first-block bits
+            uint64_t sol = 0;
+            for (uint32_t k = 0; k < j->tier_s; k++) sol |= ((p >> (j->tier_s - 1 - k)) & 1ull) << k;
+            sol |= r.solution_lo << j->tier_s;
+            j->res.has_solution = 1;
+            j->res.solution = sol;
+            finished = true;
+        } else if (j->qr) {
+            for (uint64_t k = 0; k < B && !finished; k++) {
+                j->qr->push(r.value != 0);
+                FinalResult fr;
+                if (j->qr->final_result(&fr)) {
+                    j->res.has_solution = fr.has_solution;
+                    j->res.solution = fr.has_solution ? fr.solution : 0;
+                    finished = true;
+                }
+            }
+        }
+        if (!finished && j->next_block == nblocks) finished = true;   // no decisive unit anywhere
+        if (finished) {
+            j->res.reversed = j->quants[0];
+            j->res.solution_bits = j->f;
+            j->res.value = j->res.has_solution ? (j->quants[0] ? 0 : 1) : (j->quants[0] ? 1 : 0);
+            j->finished = true;
+            j->tier_cancel = true;
+            j->tcv.notify_all();
+            break;
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_queued) {
@@ -797,17 +1011,30 @@ extern "C" int nsat_server_step(nsat_server* s, uint32_t* n_active, uint32_t* n_
         s->cur ^= 1;
     }
     s->cur ^= 1;
-    // retire finished jobs that no launched epoch still reads
+    for (auto& jp : s->active)
+        if (jp->kind == SRV_QSAT) tier_step(s, jp.get());
+    // answer and release finished jobs that no launched epoch still reads; a
+    // job a tiering worker still reads is parked until the worker lets go
     std::vector<std::unique_ptr<Job>> keep;
     for (auto& jp : s->active) {
         if (jp->finished && jp->inflight == 0) {
+            if (jp->tier.load() != TIER_NONE && !jp->tier_cancel) {
+                jp->tier_cancel = true;      // answered by the interpreter first
+                jp->tcv.notify_all();
+            }
             release(s, jp.get());
             finish(s, jp.get());
+            const int t = jp->tier.load();
+            if (t != TIER_NONE && t != TIER_DONE) s->parked.push_back(std::move(jp));
         } else {
             keep.push_back(std::move(jp));
         }
     }
     s->active.swap(keep);
+    std::vector<std::unique_ptr<Job>> still;
+    for (auto& jp : s->parked)
+        if (jp->tier.load() != TIER_DONE) still.push_back(std::move(jp));
+    s->parked.swap(still);
     if (n_active) *n_active = (uint32_t)s->active.size();
     if (n_queued) *n_queued = (uint32_t)s->queue.size();
     return NSAT_OK;

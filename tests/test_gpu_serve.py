@@ -126,3 +126,36 @@ def test_job_larger_than_arena_is_answered_with_enomem(ctx):
         exp = expected(r)
         assert res[i]["status"] == 0
         assert project(res[i], exp) == exp
+
+
+@pytest.mark.parametrize("wait", [True, False])
+def test_qsat_tiering_matches_one_shot(ctx, wait):
+    """QSAT jobs racing a compiled kernel (tier_min_ms=1 makes every large
+    one a candidate): with tier_wait every block runs compiled, without it
+    the interpreter and the compiled blocks share the job; the answers equal
+    the one-shot solver's (decisive units inside blocks, blocks inside units,
+    and formulas decided by the reducer alike)."""
+    reqs = []
+    for seed in range(8):
+        n = 28 + seed % 3
+        c = W.random_dag(500 + seed, n, 900, output="live")
+        reqs.append((c, W.alternating_quants(seed, n, 1 + seed % 5)))
+    # first blocks that reach below the tile: units smaller than a tile, no reducer
+    c = W.random_dag(600, 28, 900, output="live")
+    reqs.append((c, "E" * 25 + "AEA"))
+    reqs.append((c, "A" * 26 + "EA"))
+    srv = api.Server(ctx, tier_min_ms=1, tier_wait=wait)
+    for i, (c, q) in enumerate(reqs):
+        srv.submit("qsat", c, quants=q, tag=i)
+    res = {r["tag"]: r for r in srv.run_all()}
+    srv.close()
+    compiled = 0
+    for i, (c, q) in enumerate(reqs):
+        one = ctx.circuit(c).qsat(q)
+        got = res[i]
+        assert got["status"] == 0
+        assert (got["reversed"], got["solution_bits"], got["solution"]) == \
+            (one["reversed"], one["solution_bits"], one["solution"]), (i, got, one)
+        compiled += got["compiled_blocks"]
+    if wait:
+        assert compiled > 0
