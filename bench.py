@@ -668,6 +668,10 @@ def run_serving(args, world, rank, local):
                                "at t=0 (value) and with Poisson arrivals at %.0f/s (latency)"
                                % (len(reqs), kinds["sat"], kinds["qsat"], kinds["stop"], args.rate),
                    "step": "one request solved", "epochs": st_sat["epochs"],
+                   "qsat_tiering": {"jobs": sum(1 for r in res_sat.values() if r["compiled_blocks"]),
+                                    "compiled_blocks": sum(r["compiled_blocks"] for r in res_sat.values()),
+                                    "note": "large QSAT jobs race a kernel compiled for them; its 1/16 prefix "
+                                            "blocks take over once it is ready"},
                    "l2": "no memory inputs (assignments come from thread indices)"},
         "latency": dict(poi_sum, rate_hz=args.rate, epochs=st_poi["epochs"]),
         "plain": {"form": "one request at a time through the one-shot solvers (per-circuit NVRTC kernel, "
@@ -693,7 +697,8 @@ def run_serving(args, world, rank, local):
                 "d2h_bytes_per_step": st_sat["d2h_bytes"] / len(reqs),
                 "note": "the server runs end to end: circuits arrive as host arrays, programs and epoch tables "
                         "are copied in, results copied out; bytes per request from the server's counters"},
-        "gpu_launches": st_sat["launches"],
+        # interpreter epochs and join rounds, plus at least one launch per compiled block
+        "gpu_launches": st_sat["launches"] + sum(r["compiled_blocks"] for r in res_sat.values()),
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
