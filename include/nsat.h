@@ -306,8 +306,8 @@ typedef struct {
                                    (about 30 ms of device time; on the config-4 trace smaller
                                    budgets raise p99 and lower solves/s) */
     uint32_t build_threads;     /* host threads that build job programs; 0 = min(8, cores / 2) */
-    uint32_t tier_threads;      /* QSAT tiering workers (own context each); 0 = half the host
-                                   threads, between 2 and 12 */
+    uint32_t tier_threads;      /* QSAT tiering workers (own context each); 0 = three quarters of
+                                   the host threads, between 2 and 12 */
     uint32_t tier_min_ms;       /* QSAT jobs whose whole index space would take the interpreter
                                    longer than this (estimate) race a compiled kernel: it is
                                    compiled in the background and, once ready, solves the job's

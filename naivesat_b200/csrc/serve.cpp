@@ -239,6 +239,7 @@ struct Job {
     std::atomic<int> tier{0};            // TIER_* below
     std::atomic<bool> tier_cancel{false};
     std::atomic<int64_t> run_from{-1};   // first block the worker solves (set by step)
+    double tier_est_ms = 0;              // interpreter estimate for the whole job (queue priority)
     uint32_t tier_s = 0;                 // prefix bits of a block
     uint64_t tier_block = 0;             // tiles per block
     uint64_t stop_at = UINT64_MAX;       // the interpreter stops at this tile
@@ -544,6 +545,7 @@ void builder_loop(nsat_server* s, bool raw) {
             s->tier_enabled) {
             const double est_ms = std::ldexp(1.0, (int)j->nb - 5) * (double)j->prog.ins.size() / kInterpRate * 1e3;
             if (est_ms > (double)s->opts.tier_min_ms) {
+                j->tier_est_ms = est_ms;
                 j->tier_s = 4;
                 j->tier_block = j->total_tiles >> j->tier_s;
                 j->tier = TIER_COMPILING;
@@ -577,8 +579,12 @@ void tier_loop(nsat_server* s, nsat_opts copts) {
             std::unique_lock<std::mutex> lk(s->tqmu);
             s->tqcv.wait(lk, [s] { return s->tstop.load() || !s->tqueue.empty(); });
             if (s->tstop) break;
-            j = s->tqueue.front();
-            s->tqueue.pop_front();
+            // the largest estimated job first: one compile saves the most interpreter time there
+            auto best = s->tqueue.begin();
+            for (auto it = s->tqueue.begin(); it != s->tqueue.end(); ++it)
+                if ((*it)->tier_est_ms > (*best)->tier_est_ms) best = it;
+            j = *best;
+            s->tqueue.erase(best);
         }
         if (!wctx || j->tier_cancel) {
             j->tier = TIER_DONE;
@@ -678,10 +684,12 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     SCK(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
     SCK(cudaMalloc(&s->d_join, sizeof(NsatJoinState)));
     SCK(cudaMallocHost(&s->h_join, sizeof(NsatJoinState)));
-    // defaults measured on the config-4 trace (3000 requests): 30 ms and 8
-    // workers took 366 -> 609 solves/s and p99 at 150/s 172 -> 42 ms
+    // defaults measured on the config-4 trace: 30 ms and 8 workers took a
+    // 3000-request prefix from 366 to 609 solves/s (p99 at 150/s 172 -> 42 ms);
+    // on all 10,000 requests, 12 workers (the compiles are the limit) reach
+    // 517 solves/s against 435 with 8
     if (s->opts.tier_min_ms == 0) s->opts.tier_min_ms = 30;
-    const uint32_t hw_tier = std::max(2u, std::min(12u, std::thread::hardware_concurrency() / 2));
+    const uint32_t hw_tier = std::max(2u, std::min(12u, std::thread::hardware_concurrency() * 3 / 4));
     const uint32_t ntier =
         s->opts.tier_min_ms == 0xffffffffu ? 0 : (s->opts.tier_threads ? s->opts.tier_threads : hw_tier);
     s->tier_enabled = ntier > 0;
