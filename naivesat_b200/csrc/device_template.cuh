@@ -117,12 +117,33 @@ __device__ __forceinline__ u32 decisive(u32 y, int k, int nodes) {
     return (NSAT_Q0ALL ? ~y : y) & unit_mask(k) & valid;
 }
 
+// number of consecutive levels from level 0 that share level 0's quantifier
+__device__ constexpr int low_run(u64 allbits) {
+    int k = 1;
+    while (k < 64 && (((allbits >> k) ^ allbits) & 1ull) == 0ull) k++;
+    return k;
+}
+
 extern "C" __global__ void NSAT_BOUNDS
 nsat_qsat(u64 launch, LaunchOut* __restrict__ out, unsigned char* __restrict__ scratch,
           const u32* __restrict__ data) {
     constexpr int M = NSAT_M;
-    constexpr int G1 = NSAT_IT < 5 ? NSAT_IT : 5;
-    constexpr int G2 = NSAT_IT - G1;
+    // Folding.  When levels 0..9 (the word and the warp tile) and the lowest
+    // FOLD iteration levels all carry level 0's quantifier and lie below the
+    // units, their nodes are one AND (or OR) over 2^(10+FOLD) items, taken in
+    // any order: a thread combines its words over 2^FOLD iterations with one
+    // op per word, and a compare plus a warp vote gives the node at level
+    // L0 = 10+FOLD.  Otherwise the word and tile trees run per iteration and
+    // L0 = 10.  Stage 2 reduces the IT2 = IT-FOLD remaining iteration levels.
+    constexpr int QLOW = low_run(NSAT_ALLBITS);
+    constexpr bool FOLDED = M >= 10 && QLOW >= 10;
+    constexpr int FOLD_CAP = QLOW < M ? QLOW : M;
+    constexpr int FOLD = !FOLDED ? 0 : (FOLD_CAP < 10 + NSAT_IT ? FOLD_CAP : 10 + NSAT_IT) - 10;
+    constexpr bool LOW_ALL = (NSAT_ALLBITS & 1ull) != 0ull;
+    constexpr int L0 = 10 + FOLD;
+    constexpr int IT2 = NSAT_IT - FOLD;
+    constexpr int G1 = IT2 < 5 ? IT2 : 5;
+    constexpr int G2 = IT2 - G1;
     const u32 lane = threadIdx.x & 31u;
     const u32 warp = threadIdx.x >> 5;
     const u32 cta = blockIdx.x;
@@ -134,6 +155,7 @@ nsat_qsat(u64 launch, LaunchOut* __restrict__ out, unsigned char* __restrict__ s
 #endif
     u64 cand = ~0ull;      // lowest decisive unit seen by this thread (launch-relative)
     u32 acc1 = 0, acc2 = 0;
+    u32 yacc = LOW_ALL ? 0xffffffffu : 0u;
     for (u32 it = 0; it < (1u << NSAT_IT); it++) {
 #if NSAT_DATA
         const u64 gw = ((u64)launch << (NSAT_C - 5)) + ((warp_base + ((u64)it << 10)) >> 5) + lane;
@@ -142,61 +164,72 @@ nsat_qsat(u64 launch, LaunchOut* __restrict__ out, unsigned char* __restrict__ s
         nsat_inputs_iter(x, it);
         u32 y = nsat_eval1(x);
 #endif
-        const u64 tile_base = warp_base + ((u64)it << 10);   // first item of this warp tile
-        // stage 0: the 32 lanes of the word (levels 0..4)
-        if constexpr (M < 5) {
-            y = tree_up<0, M>(y);
-            const u32 d = decisive(y, M, 32);
-            if (d != 0u && cand == ~0ull)
-                cand = ((tile_base + ((u64)lane << 5)) >> M) + (u64)((__ffs(d) - 1) >> M);
-            continue;
+        u32 b, git;   // node value at level L0 (bit 0) and its index among the warp's L0 nodes
+        if constexpr (FOLDED) {
+            yacc = LOW_ALL ? (yacc & y) : (yacc | y);
+            if (((it + 1u) & ((1u << FOLD) - 1u)) != 0u) continue;
+            const bool v = LOW_ALL ? (yacc == 0xffffffffu) : (yacc != 0u);
+            yacc = LOW_ALL ? 0xffffffffu : 0u;
+            b = LOW_ALL ? (u32)__all_sync(0xffffffffu, v) : (u32)__any_sync(0xffffffffu, v);
+            git = it >> FOLD;
         } else {
-            y = tree_up<0, 5>(y);
+            const u64 tile_base = warp_base + ((u64)it << 10);   // first item of this warp tile
+            // stage 0: the 32 lanes of the word (levels 0..4)
+            if constexpr (M < 5) {
+                y = tree_up<0, M>(y);
+                const u32 d = decisive(y, M, 32);
+                if (d != 0u && cand == ~0ull)
+                    cand = ((tile_base + ((u64)lane << 5)) >> M) + (u64)((__ffs(d) - 1) >> M);
+                continue;
+            } else {
+                y = tree_up<0, 5>(y);
+            }
+            // stage 1: the 32 words of the warp tile (levels 5..9)
+            b = __ballot_sync(0xffffffffu, y & 1u);
+            if constexpr (M >= 5 && M < 10) {
+                b = tree_up<5, M - 5>(b);
+                const u32 d = decisive(b, M - 5, 32);
+                if (d != 0u && cand == ~0ull)
+                    cand = (tile_base >> M) + (u64)((__ffs(d) - 1) >> (M - 5));
+                continue;
+            } else {
+                b = tree_up<5, 5>(b);
+            }
+            git = it;
         }
-        // stage 1: the 32 words of the warp tile (levels 5..9)
-        u32 b = __ballot_sync(0xffffffffu, y & 1u);
-        if constexpr (M >= 5 && M < 10) {
-            b = tree_up<5, M - 5>(b);
-            const u32 d = decisive(b, M - 5, 32);
-            if (d != 0u && cand == ~0ull)
-                cand = (tile_base >> M) + (u64)((__ffs(d) - 1) >> (M - 5));
-            continue;
-        } else {
-            b = tree_up<5, 5>(b);
-        }
-        // stage 2: iterations of the warp's loop (levels 10..10+IT-1)
-        if constexpr (M >= 10 && NSAT_IT > 0) {
-            const u32 pos = it & ((1u << G1) - 1u);
+        // stage 2: the warp's L0 nodes (levels L0..10+IT-1), 2^G1 at a time
+        if constexpr (M >= L0 && IT2 > 0) {
+            const u32 pos = git & ((1u << G1) - 1u);
             acc1 |= (b & 1u) << pos;
             if (pos == (1u << G1) - 1u) {
-                const u64 grp_base = tile_base - ((u64)pos << 10);
-                if constexpr (M < 10 + G1) {
-                    const u32 y1 = tree_up<10, M - 10>(acc1);
-                    const u32 d = decisive(y1, M - 10, 1 << G1);
+                const u64 grp_base = warp_base + ((u64)(git - pos) << L0);
+                if constexpr (M < L0 + G1) {
+                    const u32 y1 = tree_up<L0, M - L0>(acc1);
+                    const u32 d = decisive(y1, M - L0, 1 << G1);
                     if (d != 0u && cand == ~0ull)
-                        cand = (grp_base >> M) + (u64)((__ffs(d) - 1) >> (M - 10));
+                        cand = (grp_base >> M) + (u64)((__ffs(d) - 1) >> (M - L0));
                 } else {
-                    const u32 y1 = tree_up<10, G1>(acc1);
-                    acc2 |= (y1 & 1u) << (it >> G1);
+                    const u32 y1 = tree_up<L0, G1>(acc1);
+                    acc2 |= (y1 & 1u) << (git >> G1);
                 }
                 acc1 = 0;
             }
-        } else if constexpr (M >= 10) {
-            acc2 = b & 1u;   // IT == 0: the tile is the warp's whole range
+        } else if constexpr (M >= L0) {
+            acc2 = b & 1u;   // IT2 == 0: one L0 node is the warp's whole range
         }
     }
-    // stage 2b: groups of iterations (levels 10+G1 .. 10+IT-1)
+    // stage 2b: groups of L0 nodes (levels L0+G1 .. 10+IT-1)
     u32 wres = 0;
-    if constexpr (M >= 10 + G1 && NSAT_IT > 0) {
-        if constexpr (M < 10 + NSAT_IT) {
-            const u32 y2 = tree_up<10 + G1, M - 10 - G1>(acc2);
-            const u32 d = decisive(y2, M - 10 - G1, 1 << G2);
+    if constexpr (M >= L0 + G1 && IT2 > 0) {
+        if constexpr (M < L0 + IT2) {
+            const u32 y2 = tree_up<L0 + G1, M - L0 - G1>(acc2);
+            const u32 d = decisive(y2, M - L0 - G1, 1 << G2);
             if (d != 0u && cand == ~0ull)
-                cand = (warp_base >> M) + (u64)((__ffs(d) - 1) >> (M - 10 - G1));
+                cand = (warp_base >> M) + (u64)((__ffs(d) - 1) >> (M - L0 - G1));
         } else {
-            wres = tree_up<10 + G1, G2>(acc2) & 1u;
+            wres = tree_up<L0 + G1, G2>(acc2) & 1u;
         }
-    } else if constexpr (M >= 10 && NSAT_IT == 0) {
+    } else if constexpr (M >= L0 && IT2 == 0) {
         wres = acc2 & 1u;
     }
     // per-warp lowest candidate, one atomic per warp

@@ -367,6 +367,16 @@ int or_qr_push(or_qr* qr, uint64_t index, int item) {
     return 0;
 }
 
+/* the items of packed words (item k = bit k%32 of word k/32), in index order,
+ * until the reducer is final; test helper for the device reduction */
+int or_qr_push_words(or_qr* qr, const uint32_t* words, uint64_t nwords) {
+    for (uint64_t k = 0; k < nwords * 32u; k++) {
+        if (qr_is_end(qr) || qr->has_solution) break;
+        if (or_qr_push(qr, k, (int)((words[k >> 5] >> (k & 31u)) & 1u))) return -1;
+    }
+    return 0;
+}
+
 int or_qr_final(const or_qr* qr, int* reversed, uint32_t* solution_bits,
                 int* has_solution, uint64_t* solution) {
     if (!(qr_is_end(qr) || qr->has_solution)) return 0;

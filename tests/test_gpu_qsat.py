@@ -2,7 +2,9 @@
 known answers, through the C ABI."""
 import json
 import os
+import random
 
+import numpy as np
 import pytest
 
 from naivesat_b200 import workloads as W
@@ -72,6 +74,51 @@ def test_qsat_random_matches_oracle(ctx, t):
     # small launches: the host QuantReducer joins per-launch results
     got2 = ctx.circuit(c).qsat(q, chunk_bits=15)
     assert strip(got2) == exp
+
+
+def _block_data(rng, n, q):
+    """Words whose innermost quantifier block (the last run of equal letters,
+    item bit 0 = last quantifier) gets node values about half true: per node,
+    one set bit (Exists) or one cleared bit (All) with probability 1/2."""
+    L = 1
+    while L < n and q[n - 1 - L] == q[-1]:
+        L += 1
+    words = np.full((1 << n) // 32, 0xFFFFFFFF if q[-1] == "A" else 0, dtype=np.uint32)
+    for node in range(1 << (n - L)):
+        if rng.random() < 0.5:
+            k = (node << L) + rng.randrange(1 << L)
+            words[k >> 5] ^= np.uint32(1 << (k & 31))
+    return words
+
+
+# (n, quantifiers): long innermost blocks fold words over iterations (the
+# launch has n - 25 iteration bits): fold of every iteration level, of some
+# with the rest reduced per node, units right at the fold level, a fold of
+# zero levels (only levels 0..9 alike), units two nodes above the fold,
+# and one of each innermost letter.
+FOLD_CASES = [(26, "A" + "E" * 25), (26, "E" + "A" * 25), (26, "EEAAA" + "E" * 21),
+              (27, "E" * 15 + "A" + "E" * 11), (27, "A" * 16 + "E" * 11),
+              (27, "AE" * 6 + "E" + "A" * 14), (27, "E" * 16 + "A" * 11), (26, "EAE" + "A" * 13 + "E" * 10),
+              (25, "A" * 5 + "E" * 20), (24, "EA" * 7 + "A" * 10), (28, "E" * 16 + "A" + "E" * 11)]
+
+
+@pytest.mark.parametrize("case", range(len(FOLD_CASES)))
+def test_reduce_words_folded_blocks(ctx, case):
+    n, q = FOLD_CASES[case]
+    rng = random.Random(4200 + case)
+    for _ in range(3):
+        w = _block_data(rng, n, q)
+        qr = O.QuantReducer(q)
+        qr.push_words(w)
+        assert strip(ctx.qsat_reduce_words(q, w)) == qr.final_result(), (n, q)
+
+
+@pytest.mark.parametrize("q", ["A" + "E" * 27, "E" * 2 + "A" * 12 + "E" * 14, "E" * 5 + "A" * 11 + "E" * 12,
+                               "A" * 3 + "E" * 14 + "A" * 11, "E" * 16 + "A" + "E" * 11])
+def test_qsat_folded_blocks_match_oracle(ctx, q):
+    c = W.random_dag(41, 28, 300, output="live")
+    exp = O.qsat(O.Circuit(c.n, c.gates, c.outputs), q, mode=1)
+    assert strip(ctx.circuit(c).qsat(q)) == exp, q
 
 
 def test_qsat_all_same_quantifier(ctx):

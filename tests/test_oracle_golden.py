@@ -41,6 +41,25 @@ def test_quant_reducer_kat(i):
     assert qr.final_result() == c["result"]
 
 
+def test_quant_reducer_push_words_kat():
+    """The packed-word push (items in index order) gives the reference's
+    final results on the test_quant_reducer cases of >= 32 items."""
+    n = 0
+    for c in load("quant_reducer.json"):
+        nq = len(c["quants"])
+        if nq < 5:
+            continue
+        words = [0] * ((1 << nq) // 32)
+        for k, it in enumerate(c["items"]):
+            if it:
+                words[k >> 5] |= 1 << (k & 31)
+        qr = O.QuantReducer(c["quants"])
+        qr.push_words(words)
+        assert qr.final_result() == c["result"], c
+        n += 1
+    assert n >= 10
+
+
 def test_aggr_tree_cpu_kat():
     """qsat.rs test_aggr_output_cpu_code: quantifier tree over word bits."""
     for c in load("aggr_tree_cpu.json"):
