@@ -8,7 +8,7 @@ namespace nsat {
 
 std::string KernelConfig::key() const {
     std::ostringstream s;
-    s << "mode=" << (int)mode << " nin=" << nin << " it=" << it << " wb=" << wb << " cb=" << cb
+    s << "mode=" << (int)mode << " nin=" << nin << " nb=" << nb << " c=" << c << " it=" << it << " wb=" << wb << " cb=" << cb
       << " m=" << m << " q0all=" << q0all << " allbits=" << allbits << " data=" << data
       << " fmt=" << fmt << " nout=" << nout << " minb=" << minb << " sync=" << sync_every << " map=";
     for (int v : in_of_bit) s << v << ',';

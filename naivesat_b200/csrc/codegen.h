@@ -29,7 +29,7 @@ struct KernelConfig {
     uint32_t nout = 1;
 
     uint32_t threads() const { return 32u << wb; }
-    std::string key() const;   // compact description for cache keys/logs
+    std::string key() const;   // every field the generated source depends on (with the LUT net)
 };
 
 // Full NVRTC source: prelude, generated input/eval functions, template.

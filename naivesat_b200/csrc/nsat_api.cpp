@@ -84,6 +84,9 @@ struct nsat_circuit {
     nsat_ctx* ctx = nullptr;
     Circuit circ;
     std::map<std::string, LutNet> nets;
+    // kernels loaded for this handle, by net key + kernel config + entry
+    // point: a repeated solve skips generating and hashing the source
+    std::map<std::string, std::pair<CUfunction, std::shared_ptr<JitModule>>> kernels;
     Shape tuned;                 // set by nsat_autotune (per kind)
     Shape tuned_qsat;
 };
@@ -144,9 +147,14 @@ Circuit from_desc(const nsat_circuit_desc* d) {
     return c;
 }
 
-const LutNet& get_net(nsat_circuit* c, const std::vector<uint32_t>& which) {
+std::string net_key(const nsat_circuit* c, const std::vector<uint32_t>& which) {
     std::string key = c->ctx->opts.no_optimize ? "raw:" : "lut:";
     for (uint32_t j : which) key += std::to_string(j) + ",";
+    return key;
+}
+
+const LutNet& get_net(nsat_circuit* c, const std::vector<uint32_t>& which) {
+    const std::string key = net_key(c, which);
     auto it = c->nets.find(key);
     if (it != c->nets.end()) return it->second;
     return c->nets[key] = map_luts(c->circ, which, c->ctx->opts.no_optimize != 0);
@@ -209,6 +217,22 @@ int get_kernel(nsat_ctx* ctx, const KernelConfig& kc, const LutNet& net, const c
     if (rc == -3) return fail(ctx, NSAT_ECOMPILE, err);
     if (rc != 0) return fail(ctx, NSAT_ECUDA, err);
     *fn = (*holder)->fns[name];
+    return NSAT_OK;
+}
+
+// get_kernel through the circuit handle's kernel map.
+int get_circuit_kernel(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint32_t>& which,
+                       const KernelConfig& kc, const LutNet& net, const char* name, CUfunction* fn,
+                       std::shared_ptr<JitModule>* holder) {
+    const std::string key = net_key(c, which) + "|" + kc.key() + "|" + name;
+    auto it = c->kernels.find(key);
+    if (it != c->kernels.end()) {
+        *fn = it->second.first;
+        *holder = it->second.second;
+        return NSAT_OK;
+    }
+    if (int rc = get_kernel(ctx, kc, net, name, fn, holder)) return rc;
+    c->kernels[key] = {*fn, *holder};
     return NSAT_OK;
 }
 
@@ -574,7 +598,7 @@ extern "C" int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opt
     const u128 bp = plan.bp, ep = plan.ep;
     CUfunction fn;
     std::shared_ptr<JitModule> mod;
-    if (int rc = get_kernel(ctx, kc, net, "nsat_sat", &fn, &mod)) return rc;
+    if (int rc = get_circuit_kernel(ctx, c, out0, kc, net, "nsat_sat", &fn, &mod)) return rc;
     const uint64_t L0 = (uint64_t)(bp >> C);
     const uint64_t nl = (uint64_t)((ep - bp) >> C);
     const unsigned grid = 1u << kc.cb, threads = kc.threads();
@@ -655,7 +679,9 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     const uint64_t L0 = s ? (prefix << A) : 0;
     CUfunction fn;
     std::shared_ptr<JitModule> mod;
-    if (int rc = get_kernel(ctx, kc, net, "nsat_qsat", &fn, &mod)) return rc;
+    if (int rc = data ? get_kernel(ctx, kc, net, "nsat_qsat", &fn, &mod)
+                      : get_circuit_kernel(ctx, c, out0, kc, net, "nsat_qsat", &fn, &mod))
+        return rc;
     if (fixed_scratch) {
         if (((size_t)2 << kc.cb) > fixed_scratch_bytes)
             return fail(ctx, NSAT_EUNSUPPORTED,
@@ -823,7 +849,7 @@ extern "C" int nsat_stop_table_build(nsat_ctx* ctx, nsat_circuit* c, const nsat_
     const LutNet& net = get_net(c, which);
     CUfunction fn;
     std::shared_ptr<JitModule> mod;
-    if (int rc = get_kernel(ctx, kc, net, "nsat_table", &fn, &mod)) return rc;
+    if (int rc = get_circuit_kernel(ctx, c, which, kc, net, "nsat_table", &fn, &mod)) return rc;
     uint64_t nwords = n >= 5 ? (t->N >> 5) : 1;
     const unsigned threads = kc.threads();
     uint64_t want = (nwords + threads - 1) / threads;
@@ -863,7 +889,7 @@ int table_chunk_u64(nsat_ctx* ctx, nsat_circuit* c, uint64_t first_state, uint64
     const LutNet& net = get_net(c, which);
     CUfunction fn;
     std::shared_ptr<JitModule> mod;
-    if (int rc = get_kernel(ctx, kc, net, "nsat_table", &fn, &mod)) return rc;
+    if (int rc = get_circuit_kernel(ctx, c, which, kc, net, "nsat_table", &fn, &mod)) return rc;
     uint64_t nwords = count >> 5, w0 = first_state >> 5;
     const unsigned threads = kc.threads();
     const uint64_t want = (nwords + threads - 1) / threads;
