@@ -104,6 +104,15 @@ def test_lut_mapping_saves_ops():
     assert fused["lop3_ops"] < 0.8 * fused["live_gates"], fused
 
 
+@pytest.mark.parametrize("name,kind,lop3", [("c0", "sat", 182), ("c1", "sat", 1648), ("c1_twin", "sat", 1664),
+                                            ("c2a", "qsat", 38), ("c2c", "qsat", 731)])
+def test_lut_counts_of_the_benchmark_circuits(name, kind, lop3):
+    """The mapper is deterministic; these covers are the ones the measured
+    rooflines count."""
+    c = W.config(name)
+    assert api.jit_check(c, kind, quants=c.quants)["lop3_ops"] == lop3
+
+
 @pytest.mark.parametrize("seed,n,g,out", [(0, 24, 500, "last"), (1, 36, 3000, "live"), (3, 30, 1500, "live"),
                                           (77, 18, 100, "last"), (123456789, 34, 4000, "live")])
 def test_library_generator_matches_python(seed, n, g, out):
