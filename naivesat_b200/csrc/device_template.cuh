@@ -72,9 +72,30 @@ nsat_sat(u64 launch, LaunchOut* __restrict__ out) {
     }
     idx = warp_min_u64(idx);
     cnt = __reduce_add_sync(0xffffffffu, cnt);
-    if (lane == 0 && cnt != 0u) {
-        atomicAdd(&out->count, (u64)cnt);
-        atomicMin(&out->min_idx, idx);
+    if constexpr (NSAT_NT == 32) {
+        if (lane == 0 && cnt != 0u) {
+            atomicAdd(&out->count, (u64)cnt);
+            atomicMin(&out->min_idx, idx);
+        }
+    } else {
+        // one pair of atomics per CTA: launches with few iterations per warp
+        // would otherwise queue every warp on the same two addresses
+        // (a CTA counts at most 2^(10+IT+WB) <= 2^25 solutions)
+        constexpr int NW = NSAT_NT / 32;
+        __shared__ u64 s_idx[NW];
+        __shared__ u32 s_cnt[NW];
+        if (lane == 0) { s_idx[warp] = idx; s_cnt[warp] = cnt; }
+        __syncthreads();
+        if (warp == 0) {
+            u64 ci = lane < (u32)NW ? s_idx[lane] : ~0ull;
+            u32 cc = lane < (u32)NW ? s_cnt[lane] : 0u;
+            ci = warp_min_u64(ci);
+            cc = __reduce_add_sync(0xffffffffu, cc);
+            if (lane == 0 && cc != 0u) {
+                atomicAdd(&out->count, (u64)cc);
+                atomicMin(&out->min_idx, ci);
+            }
+        }
     }
 }
 #endif
