@@ -20,12 +20,6 @@ namespace {
 const char* kPrelude = R"NSAT(
 typedef unsigned int u32;
 typedef unsigned long long u64;
-template <int LUT>
-__device__ __forceinline__ u32 lop3(u32 a, u32 b, u32 c) {
-    u32 d;
-    asm("lop3.b32 %0, %1, %2, %3, %4;" : "=r"(d) : "r"(a), "r"(b), "r"(c), "n"(LUT));
-    return d;
-}
 )NSAT";
 
 const uint32_t kLanePat[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
@@ -37,11 +31,15 @@ const uint32_t kLanePat[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u
 // for kernels whose every thread runs the same number of evaluations.
 void emit_luts(std::ostringstream& s, const LutNet& net, uint32_t sync_every = 0) {
     for (uint32_t i : net.used_inputs) s << "    const u32 w" << i << " = x[" << i << "];\n";
-    char buf[160];
+    char buf[256];
     uint32_t k = 0;
+    // one lop3.b32 per LUT, the truth table as its immediate; written as
+    // inline asm in place (a helper template per call site costs NVVM about
+    // twice the compile time on circuits of a few thousand gates)
     for (const Lut& L : net.luts) {
-        snprintf(buf, sizeof(buf), "    const u32 w%u = lop3<0x%02x>(w%u, w%u, w%u);\n", L.wire,
-                 L.tt, L.in[0], L.in[1], L.in[2]);
+        snprintf(buf, sizeof(buf),
+                 "    u32 w%u; asm(\"lop3.b32 %%0, %%1, %%2, %%3, 0x%02x;\" : \"=r\"(w%u) : \"r\"(w%u), \"r\"(w%u), \"r\"(w%u));\n",
+                 L.wire, L.tt, L.wire, L.in[0], L.in[1], L.in[2]);
         s << buf;
         if (sync_every && ++k % sync_every == 0) s << "    __syncthreads();\n";
     }
