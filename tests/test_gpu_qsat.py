@@ -143,3 +143,27 @@ def test_qsat_config2c_matches_oracle(ctx):
     exp = O.qsat(O.Circuit(c.n, c.gates, c.outputs), c.quants, mode=1)
     got = ctx.circuit(c).qsat(c.quants)
     assert strip(got) == exp
+
+
+def test_one_handle_many_kernels(ctx):
+    """A circuit handle keeps the kernels it has loaded.  Solves of other
+    kinds, ranges, launch sizes, quantifier strings and prefixes on the same
+    handle, repeated, equal the oracle's answers (prefix solves: a fresh
+    handle's)."""
+    c = W.random_dag(77, 22, 400, output="live")
+    oc = O.Circuit(c.n, c.gates, c.outputs)
+    h = ctx.circuit(c)
+    full = O.sat_range(oc)
+    part = O.sat_range(oc, 1 << 20, 3 << 20)
+    qs = ["A" + "E" * 21, "E" * 3 + "A" * 19, W.alternating_quants(5, 22, max_block=3)]
+    exp = {q: O.qsat(oc, q, mode=1) for q in qs}
+    for _ in range(2):
+        r = h.sat()
+        assert (r["count"], r["witness"]) == full
+        r = h.sat(begin=1 << 20, end=3 << 20)
+        assert (r["count"], r["witness"]) == part
+        for q in qs:
+            assert strip(h.qsat(q)) == exp[q], q
+            assert strip(h.qsat(q, chunk_bits=16)) == exp[q], q
+            for p in range(4):
+                assert strip(h.qsat(q, prefix_bits=2, prefix=p)) == strip(ctx.circuit(c).qsat(q, prefix_bits=2, prefix=p))
