@@ -77,6 +77,8 @@ int nsat_device_count(void);
  * validates and copies the circuit; kernels are generated and NVRTC-compiled
  * lazily on first use per solve kind and cached by content hash. */
 int nsat_circuit_new(nsat_ctx* ctx, const nsat_circuit_desc* desc, nsat_circuit** out);
+/* Frees the handle and the kernels only it still holds (on its device; the
+ * caller's current device is restored).  Free circuits before their context. */
 void nsat_circuit_free(nsat_circuit* c);
 /* LUT statistics after cut mapping of output `output` (or all outputs when
  * output < 0): live two-input gates and LOP3 operations emitted. */

@@ -311,6 +311,7 @@ class CircuitHandle:
         h = C.c_void_p()
         ctx._check(lib().nsat_circuit_new(ctx.h, C.byref(d), C.byref(h)), "circuit_new")
         self.h = h
+        ctx._children.add(self)
 
     def close(self):
         if getattr(self, "h", None):

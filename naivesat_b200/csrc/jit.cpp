@@ -1,5 +1,6 @@
 // jit.cpp -- NVRTC -> cubin (sm_100a), cached in memory and on disk.
 #include "jit.h"
+#include "lru.h"
 
 #include <nvrtc.h>
 #include <sys/stat.h>
@@ -17,7 +18,28 @@ namespace nsat {
 namespace {
 
 std::mutex g_mu;
-std::map<std::pair<int, uint64_t>, std::shared_ptr<JitModule>> g_cache;   // (device, key) -> module
+// Loaded modules per device, by source key.  The count is bounded
+// (NSAT_JIT_MODULES, default 256): a long-running server compiles a kernel
+// for every large QSAT job it tiers, and each stays loaded on the GPU while
+// it is cached.  Dropping an entry unloads the module once no circuit handle
+// or running solve still holds it.
+std::map<int, LruMap<uint64_t, std::shared_ptr<JitModule>>> g_cache;
+
+size_t cache_capacity() {
+    static const size_t cap = [] {
+        const char* v = getenv("NSAT_JIT_MODULES");
+        const long n = v ? atol(v) : 0;
+        return n > 0 ? (size_t)n : (size_t)256;
+    }();
+    return cap;
+}
+
+LruMap<uint64_t, std::shared_ptr<JitModule>>& device_cache(int device) {
+    auto it = g_cache.find(device);
+    if (it == g_cache.end())
+        it = g_cache.emplace(device, LruMap<uint64_t, std::shared_ptr<JitModule>>(cache_capacity())).first;
+    return it->second;
+}
 DriverApi g_api;
 bool g_api_tried = false;
 
@@ -168,8 +190,10 @@ int jit_get(int device, const std::string& src, const std::vector<std::string>& 
     const uint64_t key = fnv(src, fnv(optstr + std::to_string(nvmaj) + "." + std::to_string(nvmin)));
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        auto it = g_cache.find({device, key});
-        if (it != g_cache.end()) { *out = it->second; return 0; }
+        if (std::shared_ptr<JitModule>* hit = device_cache(device).find(key)) {
+            *out = *hit;
+            return 0;
+        }
     }
     auto m = std::make_shared<JitModule>();
     char name[64];
@@ -212,8 +236,13 @@ int jit_get(int device, const std::string& src, const std::vector<std::string>& 
     if (verbose)
         fprintf(stderr, "[nsat] jit %s: %s regs=%d local=%dB compile=%.1fms\n", name,
                 m->from_disk ? "disk" : "nvrtc", m->regs, m->local_bytes, m->compile_ms);
-    std::lock_guard<std::mutex> lk(g_mu);
-    g_cache[{device, key}] = m;
+    // modules evicted to make room are released when this function returns:
+    // outside the lock, with this device current (the caller's contract)
+    std::vector<std::shared_ptr<JitModule>> evicted;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        device_cache(device).put(key, m, &evicted);
+    }
     *out = m;
     return 0;
 }

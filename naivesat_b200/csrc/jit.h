@@ -39,7 +39,9 @@ struct JitModule {
 };
 
 // Compiles `src` (or fetches the cubin from the caches) and loads it in the
-// current context.  `kernels` are the extern "C" names to resolve.
+// current context, which must be `device`'s.  `kernels` are the extern "C"
+// names to resolve.  A module stays loaded while the in-memory cache or a
+// holder of *out keeps it; release holders with their device current.
 int jit_get(int device, const std::string& src, const std::vector<std::string>& kernels, bool verbose,
             std::shared_ptr<JitModule>* out, std::string* err);
 

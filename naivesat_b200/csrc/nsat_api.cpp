@@ -82,6 +82,7 @@ uint32_t sync_of(const Shape& sh) { return sh.sync_every == kNoSync ? 0 : (sh.sy
 
 struct nsat_circuit {
     nsat_ctx* ctx = nullptr;
+    int device = -1;             // ctx's device (read again when the handle is freed)
     Circuit circ;
     std::map<std::string, LutNet> nets;
     // kernels loaded for this handle, by net key + kernel config + entry
@@ -280,7 +281,12 @@ int run_ring(nsat_ctx* ctx, uint64_t total, Issue issue, Consume consume, double
                                ctx->stream));
             CK(cudaEventRecord(ctx->ev0[slot], ctx->stream));
             int rc = issue(issued, slot);
-            if (rc) return rc;
+            if (rc) {
+                // earlier launches may still be queued: finish them before the
+                // caller can release the module they run from
+                cudaStreamSynchronize(ctx->stream);
+                return rc;
+            }
             CK(cudaEventRecord(ctx->ev1[slot], ctx->stream));
             CK(cudaMemcpyAsync(ctx->h_out + slot, ctx->d_out + slot, sizeof(LaunchOut), cudaMemcpyDeviceToHost,
                                ctx->stream));
@@ -513,12 +519,23 @@ extern "C" int nsat_circuit_new(nsat_ctx* ctx, const nsat_circuit_desc* desc, ns
     if (!v.empty()) return fail(ctx, NSAT_EINVAL, v);
     nsat_circuit* nc = new nsat_circuit();
     nc->ctx = ctx;
+    nc->device = ctx->device;
     nc->circ = std::move(c);
     *out = nc;
     return NSAT_OK;
 }
 
-extern "C" void nsat_circuit_free(nsat_circuit* c) { delete c; }
+extern "C" void nsat_circuit_free(nsat_circuit* c) {
+    if (!c) return;
+    // The handle may hold the last reference to its kernels' modules: release
+    // them with their device current (solves return only after their launches
+    // finished, so none is queued), then give the caller back its device.
+    int prev = -1;
+    const bool switched = cudaGetDevice(&prev) == cudaSuccess && c->device >= 0 && c->device != prev &&
+                          cudaSetDevice(c->device) == cudaSuccess;
+    delete c;
+    if (switched) cudaSetDevice(prev);
+}
 
 extern "C" int nsat_circuit_stats(nsat_ctx* ctx, nsat_circuit* c, int output, uint32_t* live,
                                   uint32_t* ops) {

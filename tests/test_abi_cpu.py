@@ -146,3 +146,18 @@ def test_server_program_check_on_config_circuits():
     for r in W.serving_requests(60, seed=3, rate_hz=1e9, n_range=(12, 22), g_range=(40, 900),
                                 stop_n_range=(8, 14)):
         api.server_program_check(r["circ"], r["kind"], seed=5)
+
+
+def test_lru_map_matches_model(tmp_path):
+    """The bounded map behind the in-memory kernel cache agrees with a plain
+    model on random finds, puts, replacements and capacity changes."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = str(tmp_path / "lru_check")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(here, "..", "naivesat_b200", "csrc"),
+                    os.path.join(here, "lru_check.cpp"), "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
