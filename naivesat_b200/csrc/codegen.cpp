@@ -31,18 +31,39 @@ const uint32_t kLanePat[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u
 // for kernels whose every thread runs the same number of evaluations.
 void emit_luts(std::ostringstream& s, const LutNet& net, uint32_t sync_every = 0) {
     for (uint32_t i : net.used_inputs) s << "    const u32 w" << i << " = x[" << i << "];\n";
-    char buf[256];
     uint32_t k = 0;
     // one lop3.b32 per LUT, the truth table as its immediate; written as
     // inline asm in place (a helper template per call site costs NVVM about
-    // twice the compile time on circuits of a few thousand gates)
+    // twice the compile time on circuits of a few thousand gates).  The lines
+    // are appended directly: the LUTs are most of the source, and formatting
+    // them through printf took most of the generation time.
+    static const char kHex[] = "0123456789abcdef";
+    auto dec = [](std::string& o, uint32_t v) {
+        char t[10];
+        int d = 0;
+        do { t[d++] = (char)('0' + v % 10); v /= 10; } while (v);
+        while (d) o.push_back(t[--d]);
+    };
+    std::string b;
+    b.reserve(net.luts.size() * 112 + (sync_every ? net.luts.size() / sync_every * 20 : 0) + 16);
     for (const Lut& L : net.luts) {
-        snprintf(buf, sizeof(buf),
-                 "    u32 w%u; asm(\"lop3.b32 %%0, %%1, %%2, %%3, 0x%02x;\" : \"=r\"(w%u) : \"r\"(w%u), \"r\"(w%u), \"r\"(w%u));\n",
-                 L.wire, L.tt, L.wire, L.in[0], L.in[1], L.in[2]);
-        s << buf;
-        if (sync_every && ++k % sync_every == 0) s << "    __syncthreads();\n";
+        b += "    u32 w";
+        dec(b, L.wire);
+        b += "; asm(\"lop3.b32 %0, %1, %2, %3, 0x";
+        b.push_back(kHex[L.tt >> 4]);
+        b.push_back(kHex[L.tt & 15]);
+        b += ";\" : \"=r\"(w";
+        dec(b, L.wire);
+        b += ") : \"r\"(w";
+        dec(b, L.in[0]);
+        b += "), \"r\"(w";
+        dec(b, L.in[1]);
+        b += "), \"r\"(w";
+        dec(b, L.in[2]);
+        b += "));\n";
+        if (sync_every && ++k % sync_every == 0) b += "    __syncthreads();\n";
     }
+    s.write(b.data(), (std::streamsize)b.size());
 }
 
 }  // namespace
