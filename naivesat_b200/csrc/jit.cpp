@@ -136,11 +136,6 @@ const DriverApi* driver_api(std::string* err) {
     return &g_api;
 }
 
-void jit_clear() {
-    std::lock_guard<std::mutex> lk(g_mu);
-    g_cache.clear();
-}
-
 namespace {
 const char* const kOpts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-lineinfo",
                              "--ptxas-options=-v", "-DNSAT_JIT=1"};

@@ -56,7 +56,5 @@ std::string jit_cache_dir();
 // FNV-1a 64 of a byte string (cache keys).
 uint64_t jit_fnv(const std::string& s);
 
-// Drops every cached module (call with the device's context current).
-void jit_clear();
 
 }  // namespace nsat
