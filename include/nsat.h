@@ -163,7 +163,8 @@ int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
  * NSAT_NOALLOC_SCRATCH_BYTES (64 KiB) inside libnsat.so instead of the
  * context's lazily allocated buffer; every GPU that loads the library holds it
  * until exit.  A solve whose launches need more scratch (2 << CB bytes, CB =
- * log2 CTAs per launch) fails with NSAT_EUNSUPPORTED; lower chunk_bits then.
+ * log2 CTAs per launch, so launches of up to 2^15 CTAs fit) fails with
+ * NSAT_EUNSUPPORTED before any kernel is compiled; lower chunk_bits then.
  * The first call on a device looks the array up (cudaGetSymbolAddress) and the
  * first call for a circuit/quantifier string compiles and loads its kernel;
  * make that first call before any stream capture.  All calls share the one
@@ -348,7 +349,12 @@ typedef struct {
     uint64_t tiles;             /* tiles evaluated by the interpreter */
     double submit_ms, admit_ms, done_ms;   /* steady clock, milliseconds */
     uint32_t compiled_blocks;   /* QSAT: prefix blocks solved by a compiled kernel (tiering) */
-    uint32_t reserved;
+    uint32_t epochs;            /* epochs that evaluated a slice of this job */
+    uint64_t first_epoch;       /* sequence number (from 1) of the first epoch that ran a slice of
+                                   this job, and of the last one; 0 when no epoch ran it.  Jobs
+                                   whose [first_epoch, last_epoch] ranges intersect shared the
+                                   device in those epochs. */
+    uint64_t last_epoch;
 } nsat_job_result;
 
 typedef struct {

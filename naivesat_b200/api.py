@@ -121,7 +121,8 @@ class JobResult(C.Structure):
                 ("solution_bits", C.c_uint32), ("has_solution", C.c_int32), ("found", C.c_int32),
                 ("solution", C.c_uint64), ("start", C.c_uint64), ("end", C.c_uint64), ("steps", C.c_uint64),
                 ("tiles", C.c_uint64), ("submit_ms", C.c_double), ("admit_ms", C.c_double),
-                ("done_ms", C.c_double), ("compiled_blocks", C.c_uint32), ("reserved", C.c_uint32)]
+                ("done_ms", C.c_double), ("compiled_blocks", C.c_uint32), ("epochs", C.c_uint32),
+                ("first_epoch", C.c_uint64), ("last_epoch", C.c_uint64)]
 
 
 class ServerStats(C.Structure):
@@ -451,7 +452,8 @@ class Server:
             for i in range(n.value):
                 r = self._buf[i]
                 d = {"id": r.id, "tag": r.tag, "status": r.status, "kind": ["sat", "qsat", "stop"][r.kind],
-                     "tiles": r.tiles, "compiled_blocks": r.compiled_blocks,
+                     "tiles": r.tiles, "compiled_blocks": r.compiled_blocks, "epochs": r.epochs,
+                     "first_epoch": r.first_epoch, "last_epoch": r.last_epoch,
                      "submit_ms": r.submit_ms, "admit_ms": r.admit_ms, "done_ms": r.done_ms}
                 if r.kind == 0:
                     d.update(satisfiable=bool(r.satisfiable), count=r.count,

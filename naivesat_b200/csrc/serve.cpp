@@ -290,6 +290,7 @@ struct nsat_server {
     NsatJoinState* d_join = nullptr;
     NsatJoinState* h_join = nullptr;
     uint64_t epochs = 0, launches = 0;
+    uint64_t launched = 0;   // epochs launched (the sequence number of the last one)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic the server issued
     double device_ms = 0;
     // builder threads: programs are built off the caller's thread
@@ -812,6 +813,13 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
     if (na) s->rr = (s->rr + 1) % na;
     b.jobs.clear();
     if (k == 0) return NSAT_OK;
+    const uint64_t seq = ++s->launched;
+    for (int c = 0; c < 2; c++)
+        for (Job* j : sel[c]) {
+            if (!j->res.first_epoch) j->res.first_epoch = seq;
+            j->res.last_epoch = seq;
+            j->res.epochs++;
+        }
     // table: narrow jobs, then wide ones
     uint32_t i = 0;
     for (int c = 0; c < 2; c++)

@@ -159,3 +159,100 @@ def test_qsat_tiering_matches_one_shot(ctx, wait):
         compiled += got["compiled_blocks"]
     if wait:
         assert compiled > 0
+
+
+def test_continuous_batching_jobs_arrive_while_others_run(ctx):
+    """Continuous batching: long jobs are put in flight first, then new SAT /
+    QSAT / SATOSTOP jobs are submitted between server steps -- four SATOSTOP
+    jobs at once while the arena has room for two of their tables, so the
+    others wait for memory -- and every result equals the oracle (the
+    one-shot solvers for the long jobs) and the same job served alone.  The
+    epoch ranges that poll returns show that the late jobs ran in the same
+    epochs as the long ones, and that the memory waiters were admitted only
+    after an earlier table was released."""
+    import time
+    longs = [{"kind": "sat", "circ": W.random_dag(800 + s, 30, 500, output="live"), "quants": None,
+              "unknowns": 0, "find_all": True} for s in range(2)]
+    qc = W.random_dag(810, 29, 400, output="live")
+    longs.append({"kind": "qsat", "circ": qc, "quants": "A" * 13 + "E" * 16, "unknowns": 0})
+    late = [r for r in small_mix(40, 75) if r["kind"] != "stop"][:14]
+    waiters = [{"kind": "stop", "circ": W.lfsr_stop(90 + s, 14, 120), "quants": None, "unknowns": 7}
+               for s in range(4)]
+    table_pair = 2 * 8 * (1 << 14)
+    srv = api.Server(ctx, arena_bytes=2 * table_pair + 192 * 1024, tier_min_ms=0xFFFFFFFF)
+    reqs, res = [], {}
+
+    def submit(r):
+        reqs.append(r)
+        srv.submit(r["kind"], r["circ"], quants=r["quants"], unknowns=r["unknowns"], tag=len(reqs) - 1,
+                   find_all=r.get("find_all", False))
+
+    def step():
+        a, q = srv.step()
+        for x in srv.poll():
+            res[x["tag"]] = x
+        return a, q
+
+    for r in longs:
+        submit(r)
+    time.sleep(0.05)                 # programs are built on the server's builder threads
+    for _ in range(3):
+        step()
+    assert not any(i in res for i in range(len(longs))), "long jobs must still be running"
+    late_tags, wait_tags = [], []
+    for k, r in enumerate(late):
+        submit(r)
+        late_tags.append(len(reqs) - 1)
+        if k == 4:
+            for w in waiters:
+                submit(w)
+                wait_tags.append(len(reqs) - 1)
+        time.sleep(0.01)
+        a, q = step()
+        if k == 4:
+            time.sleep(0.05)
+            a, q = step()
+            assert q > 0, "SATOSTOP jobs beyond the arena must wait in the queue"
+    for x in srv.run_all():
+        res[x["tag"]] = x
+    srv.close()
+    assert sorted(res) == list(range(len(reqs)))
+    assert all(res[i]["status"] == 0 for i in res)
+
+    # every answer: the oracle (small jobs) or the one-shot solvers (long jobs)
+    for i, r in enumerate(reqs):
+        if i < len(longs):
+            h = ctx.circuit(r["circ"])
+            if r["kind"] == "sat":
+                one = h.sat(find_all=True)
+                assert (res[i]["count"], res[i]["witness"]) == (one["count"], one["witness"]), i
+            else:
+                one = h.qsat(r["quants"])
+                assert (res[i]["reversed"], res[i]["solution_bits"], res[i]["solution"]) == \
+                    (one["reversed"], one["solution_bits"], one["solution"]), i
+        else:
+            exp = expected(r)
+            assert project(res[i], exp) == exp, (i, r["kind"], res[i], exp)
+    # ... and the same job served alone
+    for i, r in enumerate(reqs):
+        alone = api.Server(ctx, tier_min_ms=0xFFFFFFFF)
+        alone.submit(r["kind"], r["circ"], quants=r["quants"], unknowns=r["unknowns"],
+                     find_all=r.get("find_all", False))
+        got = alone.run_all()[0]
+        alone.close()
+        keys = ("count", "satisfiable", "witness") if r["kind"] == "sat" else \
+            ("reversed", "solution_bits", "solution") if r["kind"] == "qsat" else ("found", "start", "end", "steps")
+        assert {k: got[k] for k in keys} == {k: res[i][k] for k in keys}, (i, got, res[i])
+
+    # the late jobs shared epochs with the long ones
+    def overlaps(a, b):
+        return res[a]["first_epoch"] <= res[b]["last_epoch"] and res[b]["first_epoch"] <= res[a]["last_epoch"]
+    shared = [t for t in late_tags if any(overlaps(t, L) for L in range(len(longs)))]
+    assert len(shared) >= len(late_tags) // 2, [(t, res[t]["first_epoch"], res[t]["last_epoch"]) for t in late_tags]
+    assert all(res[L]["epochs"] > 3 for L in range(2))
+    # the memory waiters: admitted after an earlier SATOSTOP job had finished and released its tables
+    done_before = sorted(res[t]["done_ms"] for t in wait_tags)
+    admitted_late = [t for t in wait_tags if res[t]["admit_ms"] >= done_before[0]]
+    assert len(admitted_late) >= 2, [(res[t]["admit_ms"], res[t]["done_ms"]) for t in wait_tags]
+    # and every waiter still ran while the long jobs were active
+    assert any(overlaps(t, L) for t in wait_tags for L in range(len(longs)))
