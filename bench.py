@@ -168,17 +168,18 @@ class SatWorkload:
                 "lop3_per_word": self.lop3, "live_gates": self.live}
 
     def cpu(self, threads, target_s=12.0):
-        from oracle import oracle as O
-        oc = O.Circuit(self.circ.n, self.circ.gates, self.circ.outputs)
-        bits = min(24, self.circ.n)
-        while True:
-            t0 = time.perf_counter()
-            O.sat_range(oc, 0, 1 << bits, threads)
-            dt = time.perf_counter() - t0
-            if dt > target_s / 3 or bits >= min(self.circ.n, 34):
-                break
-            bits += 1
-        return (1 << bits) * self.circ.num_gates / dt, "first 2^%d assignments (%.1f s)" % (bits, dt)
+        """The generated-code CPU path (oracle/cpu_codegen.py) on a bounded
+        sample, plus the oracle's interpreter on a smaller one for the factor
+        between the two."""
+        g = cpu_codegen_sat(self.circ)
+        per, span, dt = time_codegen_sample(g, threads, target_s / 3)
+        rate = per * self.circ.num_gates / dt
+        irate, isample = interpreter_rate(self.circ, threads, 3.0)
+        g.close()
+        return rate, ("generated C per circuit, %d-bit vectors, gcc -O3 -march=native, OpenMP over args of "
+                      "2^%d assignments; %s in %.1f s" % (g.vector_bits, g.e, span, dt)), \
+            {"method": "codegen", "interpreter_value": irate, "interpreter_sample": isample,
+             "codegen_over_interpreter": rate / irate}
 
 
 class QsatWorkload:
@@ -379,6 +380,52 @@ class StopPartWorkload:
         return None, "the oracle's partitioned schedule runs on packed entries one at a time; n=28 is out of reach"
 
 
+def cpu_codegen_sat(circ):
+    from oracle import cpu_codegen as CG
+    return CG.CodegenSat(circ, 24)
+
+
+def time_codegen_sample(g, threads, min_s, start_arg=0):
+    """Times whole calls of the generated SAT evaluator: args from start_arg,
+    doubling their number until one timed pass takes min_s (the whole index
+    space at most, repeated when that is faster).  Returns (assignments,
+    description, seconds)."""
+    nargs = 1 << (g.circ.n - g.e)
+    k = 1
+    while True:
+        a0 = start_arg % nargs
+        a1 = min(nargs, a0 + k)
+        reps = 0
+        t0 = time.perf_counter()
+        while True:
+            g.sat_args(a0, a1, threads)
+            reps += 1
+            dt = time.perf_counter() - t0
+            if a1 - a0 < k and dt < min_s:
+                continue          # the whole space is smaller than the sample: repeat it
+            break
+        if dt >= min_s or (a1 - a0) < k:
+            span = "%d pass(es) over args [%d, %d)" % (reps, a0, a1)
+            return reps * ((a1 - a0) << g.e), span, dt
+        k *= 2
+
+
+def interpreter_rate(circ, threads, min_s):
+    """The oracle's slot interpreter (the checker) over the first 2^k
+    assignments, k growing until a pass takes min_s / 3."""
+    from oracle import oracle as O
+    oc = O.Circuit(circ.n, circ.gates, circ.outputs)
+    bits = min(20, circ.n)
+    while True:
+        t0 = time.perf_counter()
+        O.sat_range(oc, 0, 1 << bits, threads)
+        dt = time.perf_counter() - t0
+        if dt > min_s / 3 or bits >= circ.n:
+            break
+        bits += 1
+    return (1 << bits) * circ.num_gates / dt, "first 2^%d assignments (%.1f s)" % (bits, dt)
+
+
 def make_workload(name, log2):
     if name in ("c3p", "c3p_spill"):
         return StopPartWorkload(name)
@@ -407,40 +454,42 @@ def run_reference(args, world, rank):
         sample = "full oracle solve per step"
         span = None
     else:
-        from oracle import oracle as O
+        # the reference's CPU path restated as generated C per circuit
+        # (oracle/cpu_codegen.py); each step a bounded sample of args of
+        # 2^e assignments, moving through the index space
         circ = wl.circ
-        oc = O.Circuit(circ.n, circ.gates, circ.outputs)
-        bits = 24
-        while True:
-            t0 = time.perf_counter()
-            O.sat_range(oc, 0, 1 << bits, threads)
-            dt = time.perf_counter() - t0
-            if dt > 1.0 or bits >= min(circ.n, 34):
-                break
-            bits += 1
-        bits = min(min(circ.n, 34), bits + max(0, int(round(math.log2(4.0 / max(dt, 1e-3))))))
-        span = 1 << bits
-        space = 1 << circ.n
-        for w in range(args.warmup):
-            b = (w * span) % space
-            O.sat_range(oc, b, b + span, threads)
+        g = cpu_codegen_sat(circ)
+        nargs = 1 << (circ.n - g.e)
+        t0 = time.perf_counter()
+        g.sat_args(0, 1, threads)
+        one = max(time.perf_counter() - t0, 1e-4)
+        k = max(1, min(nargs, int(4.0 / one)))     # about 4 s of work per step
+        span = k << g.e
         times = []
-        for s in range(args.steps):
-            b = (s * span) % space
+        for s in range(args.warmup + args.steps):
+            a0 = (s * k) % nargs
+            a1 = min(nargs, a0 + k)
             t0 = time.perf_counter()
-            O.sat_range(oc, b, b + span, threads)
-            times.append(time.perf_counter() - t0)
+            g.sat_args(a0, a1, threads)
+            if a1 - a0 < k:
+                g.sat_args(0, k - (a1 - a0), threads)
+            if s >= args.warmup:
+                times.append(time.perf_counter() - t0)
         rate = span * circ.num_gates * args.steps / sum(times)
-        sample = "2^%d assignments per step (of 2^%d)" % (bits, circ.n)
+        sample = ("%d args of 2^%d assignments per step (2^%.1f of 2^%d), generated C per circuit with %d-bit "
+                  "vectors, gcc -O3 -march=native, OpenMP over args" % (k, g.e, math.log2(span), circ.n,
+                                                                        g.vector_bits))
+        g.close()
     line = {"impl": "reference", "metric": wl.metric, "value": rate, "unit": wl.metric, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": (1e3 * span * wl.circ.num_gates / rate) if span else None,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "u64 bit-sliced", "data": "synthetic",
+            "dtype": "u64 bit-sliced (vector words)", "data": "synthetic",
             "config": dict(wl.describe(), cpu=cpu_model()),
             "cpu_baseline": {"value": rate, "unit": wl.metric, "cores": threads, "kind": "port",
+                             "method": "codegen" if span else "oracle",
                              "sample": sample + "; the reference's Rust/gatenative code cannot be built "
-                                                "here, so its C restatement in oracle/ runs it"},
+                                                "here, so its restatement in oracle/ runs it"},
             "e2e": {"value": rate, "unit": wl.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -509,14 +558,21 @@ def run_ours(args, world, rank, local):
     ms_step = tot_dev / steps
     value = wl.work() * steps / (tot_dev * 1e-3)
     e2e = wl.work() * steps / (tot_e2e * 1e-3)
+    cold = cold_probe(args, local) if world == 1 else None
+    if cold is not None:
+        cold["value"] = wl.work() / (cold["solve_ms"] * 1e-3)
+        cold["unit"] = wl.metric
     lps = launches / steps
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, sample = wl.cpu(threads)
+        out = wl.cpu(threads)
+        v, sample = out[0], out[1]
         if v is not None:
             cpu = {"value": v, "unit": wl.metric, "cores": threads, "kind": "port",
                    "sample": sample + ", " + cpu_model()}
+            if len(out) > 2:
+                cpu.update(out[2])
     cfg = wl.describe()
     cfg.update(extra)
     if wl.kind != "sat":
@@ -535,11 +591,54 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": wl.metric, "h2d_bytes_per_step": int(32 * lps),
                 "d2h_bytes_per_step": int(32 * lps)},
+        "e2e_cold": cold,
         "gpu_launches": launches,
         "clocks": clk,
         "warmup_s": t_warm,
     }
+    if wl.kind == "sat":
+        # the metric counts every gate of the circuit; the evaluator runs the
+        # live ones (those the output depends on), covered by fewer LUTs
+        line["live_gate_evals_per_s"] = value * wl.live / wl.circ.num_gates
+        line["live_gates"] = wl.live
     print(json.dumps(line), flush=True)
+
+
+def cold_probe(args, local):
+    """The first solve of the workload in a new process with an empty kernel
+    cache: context creation, LUT mapping, source generation, NVRTC compile,
+    module load, launches and readback.  Returns its timings (or None)."""
+    tmp = tempfile.mkdtemp(prefix="nsat_cold_")
+    env = dict(os.environ, NSAT_JIT_CACHE=tmp)
+    cmd = [sys.executable, os.path.abspath(__file__), "--cold-probe", "--workload", args.workload,
+           "--log2", str(args.log2), "--device", str(local)]
+    try:
+        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=600)
+        for line in out.stdout.splitlines()[::-1]:
+            if line.startswith("{"):
+                d = json.loads(line)
+                d["note"] = ("first solve in a new process with an empty kernel cache (NVRTC compile and "
+                             "module load included); context creation reported apart")
+                return d
+    except Exception:
+        pass
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return None
+
+
+def run_cold_probe(args):
+    from naivesat_b200 import api
+    wl = make_workload(args.workload, args.log2)
+    t0 = time.perf_counter()
+    ctx = api.Context(args.device)
+    t1 = time.perf_counter()
+    wl.setup(ctx, 1, 0)
+    r = wl.step(fresh=False)
+    t2 = time.perf_counter()
+    print(json.dumps({"context_ms": 1e3 * (t1 - t0), "solve_ms": 1e3 * (t2 - t1),
+                      "device_ms": r["device_ms"]}), flush=True)
+    ctx.close()
 
 
 # --------------------------------------------------------------------------
@@ -628,13 +727,62 @@ def run_serving(args, world, rank, local):
     for i in res_sat:
         assert serving.verdict(reqs[i]["kind"], res_sat[i]) == serving.verdict(reqs[i]["kind"], res_poi[i]), i
 
-    # the plain form: one request at a time through the one-shot solvers
-    pres, service = serving.plain_service_times(ctx, reqs, args.plain_seconds)
-    kp = len(service)
-    same = sum(serving.verdict(reqs[i]["kind"], pres[i]) == serving.verdict(reqs[i]["kind"], res_sat[i])
-               for i in pres)
-    assert same == kp, (same, kp)
-    plain_lat = serving.fifo_latencies([r["arrival_s"] for r in reqs[:kp]], service)
+    # the plain forms, one request at a time, on the first kp requests of the
+    # trace (kp: what the compile-bound form gets through in plain_seconds):
+    # compiled one-shot solvers with an empty kernel cache (a new process per
+    # circuit), the same with every kernel already in the on-disk cache, and
+    # the precompiled interpreter serving one job at a time (no batching)
+    cache_dir = tempfile.mkdtemp(prefix="nsat_plain_")
+    try:
+        pres, service = serving.plain_service_times(ctx, reqs, args.plain_seconds, cache_dir=cache_dir)
+        kp = len(service)
+        prefix = reqs[:kp]
+        wres, wservice = serving.plain_service_times(ctx, prefix, 1e9, cache_dir=cache_dir)
+    finally:
+        shutil.rmtree(cache_dir, ignore_errors=True)
+    srv = api.Server(ctx, **srv_kw)
+    ires, iservice = serving.interpreter_alone_service_times(srv, prefix)
+    srv.close()
+    # the batched server on the same requests: all queued at t=0, and Poisson
+    srv = api.Server(ctx, **srv_kw)
+    bres, blat, bmk = serving.replay_server(srv, prefix, realtime=False)
+    srv.close()
+    srv = api.Server(ctx, **srv_kw)
+    pres_b, plat_b, pmk_b = serving.replay_server(srv, prefix, realtime=True)
+    srv.close()
+    same = 0
+    for i in range(kp):
+        v = serving.verdict(reqs[i]["kind"], res_sat[i])
+        forms = (pres[i], wres[i], ires[i], bres[i], pres_b[i])
+        assert all(serving.verdict(reqs[i]["kind"], f) == v for f in forms), i
+        same += 1
+    arr = [r["arrival_s"] for r in prefix]
+    server_prefix = serving.summarize(plat_b, pmk_b, kp)
+    server_prefix["solves_per_s"] = kp / bmk
+    server_prefix["note"] = "solves/s with the requests queued at t=0; latencies under the Poisson arrivals"
+
+    def one_at_a_time(svc, form):
+        lat = serving.fifo_latencies(arr, svc)
+        sps = kp / sum(svc)
+        return {"form": form, "solves_per_s": sps,
+                "p50_ms_at_rate": serving.percentile(lat, 50) * 1e3,
+                "p99_ms_at_rate": serving.percentile(lat, 99) * 1e3,
+                "service_p50_ms": serving.percentile(svc, 50) * 1e3,
+                "service_p99_ms": serving.percentile(svc, 99) * 1e3,
+                "server_speedup": server_prefix["solves_per_s"] / sps,
+                "keeps_up_at_rate": sps > args.rate}
+    plain_forms = {
+        "requests": kp, "rate_hz": args.rate, "server": server_prefix,
+        "interpreter_alone": one_at_a_time(iservice, "the precompiled interpreter, one job per server at a "
+                                                     "time (same server options, no batching)"),
+        "compiled_warm_cache": one_at_a_time(wservice, "one-shot solvers with every kernel already in the "
+                                                       "on-disk cache (a second pass over the same requests)"),
+        "compiled_cold_cache": one_at_a_time(service, "one-shot solvers with an empty kernel cache (per-circuit "
+                                                      "NVRTC compile, as one new process per circuit)"),
+        "latency_note": "one-at-a-time forms: FIFO latencies from their measured service times under the same "
+                        "arrivals; the server: measured under those arrivals",
+        "verdicts_equal": same,
+    }
 
     # a rate the plain form sustains: both forms on the same arrivals
     low = W.serving_requests(max(8, int(args.low_rate * args.low_seconds)), seed=77, rate_hz=args.low_rate)
@@ -674,14 +822,7 @@ def run_serving(args, world, rank, local):
                                             "blocks take over once it is ready"},
                    "l2": "no memory inputs (assignments come from thread indices)"},
         "latency": dict(poi_sum, rate_hz=args.rate, epochs=st_poi["epochs"]),
-        "plain": {"form": "one request at a time through the one-shot solvers (per-circuit NVRTC kernel, "
-                          "empty kernel cache, own launches)",
-                  "requests": kp, "solves_per_s": kp / sum(service),
-                  "p50_ms_at_rate": serving.percentile(plain_lat, 50) * 1e3,
-                  "p99_ms_at_rate": serving.percentile(plain_lat, 99) * 1e3,
-                  "latency_note": "FIFO latencies from the measured service times under the same arrivals; "
-                                  "the queue grows without bound at this rate",
-                  "verdicts_equal": same},
+        "plain_forms": plain_forms,
         "low_rate": {"rate_hz": args.low_rate, "requests": len(low),
                      "server": serving.summarize(lat_low, mk_low, len(res_low)),
                      "plain": serving.summarize(plain_low_lat, sum(svc_low), len(svc_low))},
@@ -719,7 +860,12 @@ def main():
     ap.add_argument("--plain-seconds", type=float, default=60.0, help="c4: time given to the plain form")
     ap.add_argument("--low-rate", type=float, default=2.0, help="c4: a rate the plain form sustains")
     ap.add_argument("--low-seconds", type=float, default=45.0, help="c4: length of the low-rate trace")
+    ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cold_probe:
+        run_cold_probe(args)
+        return
     world, rank, local = dist_setup()
     try:
         if args.workload == "c4":

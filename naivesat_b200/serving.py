@@ -150,13 +150,19 @@ def fifo_latencies(arrivals, service):
     return lat
 
 
-def plain_service_times(ctx, reqs, time_limit_s, fresh_jit_cache=True):
+def plain_service_times(ctx, reqs, time_limit_s, fresh_jit_cache=True, cache_dir=None):
     """Solves requests one at a time (back to back) until time_limit_s;
-    returns (results by index, service time of each in s)."""
+    returns (results by index, service time of each in s).  With
+    fresh_jit_cache the kernels compile into an empty on-disk cache, as in a
+    new process; cache_dir instead names the on-disk cache to use (a second
+    pass over the same requests with the same directory finds every kernel
+    compiled: the warm-cache plain form)."""
     old = os.environ.get("NSAT_JIT_CACHE")
-    tmp = tempfile.TemporaryDirectory(prefix="nsat_plain_") if fresh_jit_cache else None
+    tmp = tempfile.TemporaryDirectory(prefix="nsat_plain_") if (fresh_jit_cache and cache_dir is None) else None
     if tmp is not None:
         os.environ["NSAT_JIT_CACHE"] = tmp.name
+    elif cache_dir is not None:
+        os.environ["NSAT_JIT_CACHE"] = cache_dir
     try:
         t0 = time.perf_counter()
         results, service = {}, []
@@ -168,9 +174,26 @@ def plain_service_times(ctx, reqs, time_limit_s, fresh_jit_cache=True):
             service.append(time.perf_counter() - s)
         return results, service
     finally:
-        if tmp is not None:
+        if tmp is not None or cache_dir is not None:
             if old is None:
                 os.environ.pop("NSAT_JIT_CACHE", None)
             else:
                 os.environ["NSAT_JIT_CACHE"] = old
+        if tmp is not None:
             tmp.cleanup()
+
+
+def interpreter_alone_service_times(srv, reqs):
+    """The precompiled interpreter without batching: one request at a time
+    through a server that holds no other job (submit, step until answered,
+    next).  Returns (results by index, service time of each in s)."""
+    results, service = {}, []
+    for i, r in enumerate(reqs):
+        s = time.perf_counter()
+        srv.submit(r["kind"], r["circ"], quants=r["quants"], unknowns=r["unknowns"], tag=i,
+                   find_all=r.get("find_all", False))
+        got = srv.run_all()
+        service.append(time.perf_counter() - s)
+        assert len(got) == 1 and got[0]["tag"] == i
+        results[i] = got[0]
+    return results, service
