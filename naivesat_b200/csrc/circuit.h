@@ -45,7 +45,8 @@ inline uint32_t gate_eval32(uint8_t f, uint32_t a, uint32_t b) {
     }
 }
 
-// gatesim text format (reconstructed; see DESIGN notes on the parser):
+// gatesim text format, reconstructed from gatesim's documentation (the crate
+// is not vendored, so no reference file pins this grammar):
 //   [quantifiers] '{' tokens '}' '(' n ')'
 // tokens are input indices or gates `and(a,b)`, `nor(a,b)`, `nimpl(a,b)`,
 // `xor(a,b)`, each optionally followed by output markers `:k` or `:kn`

@@ -21,7 +21,7 @@
 namespace {
 
 // Scratch of the QSAT last-CTA tail: one byte per CTA plus a ping-pong half
-// (2 << CB bytes per launch).  64 KiB covers launches of up to 2^14 CTAs.
+// (2 << CB bytes per launch).  64 KiB covers launches of up to 2^15 CTAs.
 // Every GPU that loads libnsat.so holds this array until the process exits.
 constexpr size_t kScratchBytes = NSAT_NOALLOC_SCRATCH_BYTES;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];

@@ -687,6 +687,11 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
         return fail(ctx, rc, perr);
     if (prefix_bits < 64 && (prefix >> prefix_bits) != 0) return fail(ctx, NSAT_EINVAL, "prefix wider than prefix_bits");
     const KernelConfig& kc = plan.kc;
+    // a launch the fixed area cannot hold is refused before any kernel is compiled or loaded
+    if (fixed_scratch && ((size_t)2 << kc.cb) > fixed_scratch_bytes)
+        return fail(ctx, NSAT_EUNSUPPORTED,
+                    "launch needs " + std::to_string((size_t)2 << kc.cb) + " scratch bytes, the fixed area holds " +
+                    std::to_string(fixed_scratch_bytes) + " (use smaller chunk_bits)");
     const std::vector<uint8_t>& q = plan.q;
     // below a fixed prefix of s inputs the problem is the sub-formula over
     // inputs s..n-1: its first block has fsub inputs and As quantifiers lie
@@ -699,13 +704,8 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
     if (int rc = data ? get_kernel(ctx, kc, net, "nsat_qsat", &fn, &mod)
                       : get_circuit_kernel(ctx, c, out0, kc, net, "nsat_qsat", &fn, &mod))
         return rc;
-    if (fixed_scratch) {
-        if (((size_t)2 << kc.cb) > fixed_scratch_bytes)
-            return fail(ctx, NSAT_EUNSUPPORTED,
-                        "launch needs " + std::to_string((size_t)2 << kc.cb) + " scratch bytes, the fixed area holds " +
-                        std::to_string(fixed_scratch_bytes) + " (use smaller chunk_bits)");
-    } else if (int rc = ensure_scratch(ctx, (size_t)2 << kc.cb)) {
-        return rc;
+    if (!fixed_scratch) {
+        if (int rc = ensure_scratch(ctx, (size_t)2 << kc.cb)) return rc;
     }
     if (data) {
         // expand 2^n items to 2^np (each item repeated 2^d times)

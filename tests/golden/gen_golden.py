@@ -3,7 +3,7 @@
 
 Run once in a container that has the reference source tree; the fixtures it
 writes next to this script are committed, and nothing at test time reads the
-reference.  Usage:  python tests/golden/gen_golden.py [REFERENCE_ROOT]
+reference.  Usage:  python tests/golden/gen_golden.py REFERENCE_ROOT
 
 The reference keeps its test vectors as Rust literals inside `#[cfg(test)]`
 modules.  This script tokenises those literal arrays with a small expression
@@ -368,7 +368,9 @@ def final_result(d):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        raise SystemExit("usage: gen_golden.py <root of the reference's source tree>")
+    ref = sys.argv[1]
     qsat = open(os.path.join(ref, "src/qsat.rs")).read()
     greedy = open(os.path.join(ref, "src/greedysatostop.rs")).read()
     out = {}

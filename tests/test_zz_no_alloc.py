@@ -37,6 +37,17 @@ def test_noalloc_matches_allocating_solve_twice():
                 assert {k: got[k] for k in KEYS} == {k: ref[k] for k in KEYS}, (circ.name, quants, call)
 
 
+def test_noalloc_boundary_launch_of_2_15_ctas():
+    # one-warp CTAs over 2^35 assignments per launch: 2^15 CTAs, whose tail
+    # needs 2 << 15 bytes, exactly the fixed area
+    with api.Context(0, block_threads=32) as ctx:
+        h = ctx.circuit(W.config("c1"))
+        ref = h.qsat("E" * 36, chunk_bits=35)
+        for call in range(2):
+            got = h.qsat_noalloc("E" * 36, chunk_bits=35)
+            assert {k: got[k] for k in KEYS} == {k: ref[k] for k in KEYS}, call
+
+
 def test_noalloc_rejects_launches_beyond_the_fixed_area():
     # one-warp CTAs over 2^36 assignments per launch need 2^16 CTAs:
     # 2 << 16 = 128 KiB of scratch > 64 KiB
