@@ -99,6 +99,23 @@ int nsat_format(const nsat_circuit_desc* desc, const uint8_t* quants, char* buf,
 /* Replaces do_command_with_{par,opencl,parseq}_mapper with AGGR_OUTPUT_*_CODE
  * (main.rs:76-264).  Natural order: input b is bit b of the assignment index.
  * Output 0 of the circuit is the formula. */
+/* A chunk queue shared by several concurrent solves of one SAT search, one
+ * context per device, each on its own host thread: the counterpart of the
+ * reference's ParSeq mapper, which hands args to whichever device is free and
+ * stops every device once one holds a witness (main.rs:205-264).
+ * Zero-initialise one, then give the same object, range and chunk_bits to
+ * every participant's nsat_sat_solve (find_all = 0).  Participants claim
+ * chunks (launches) in increasing order with an atomic counter; a chunk
+ * holding a solution lowers `stop_plus1`, and nobody claims a chunk at or
+ * above it.  Every chunk below the final stop is evaluated by some
+ * participant, so the lowest of their witnesses is the range's lowest.
+ * Accessed with host atomics only; it must outlive the solves. */
+typedef struct {
+    uint64_t next;         /* next chunk to claim, counted from the range's start */
+    uint64_t stop_plus1;   /* 0, or 1 + the lowest chunk known to hold a solution */
+    uint64_t reserved[6];
+} nsat_sat_share;
+
 typedef struct {
     uint32_t find_all;     /* 0: stop after the first chunk holding a solution and
                               return the lowest one (naivesat); 1: scan the
@@ -107,6 +124,9 @@ typedef struct {
                               reference's -e elem_inputs maps here */
     uint64_t begin_lo, begin_hi;  /* first index of the range (chunk aligned) */
     uint64_t end_lo, end_hi;      /* end of range; both 0 = 2^n */
+    nsat_sat_share* share;        /* NULL, or the queue of a search split over
+                                     several contexts (find_all must be 0); the
+                                     result then covers this context's chunks */
 } nsat_sat_opts;
 
 typedef struct {

@@ -32,10 +32,16 @@ class Opts(C.Structure):
                 ("verbose", C.c_uint32), ("min_blocks", C.c_uint32)]
 
 
+class SatShare(C.Structure):
+    """nsat_sat_share: the chunk queue of one SAT search split over several
+    contexts (zero-initialised; pass the same object to every solve)."""
+    _fields_ = [("next", C.c_uint64), ("stop_plus1", C.c_uint64), ("reserved", C.c_uint64 * 6)]
+
+
 class SatOpts(C.Structure):
     _fields_ = [("find_all", C.c_uint32), ("chunk_bits", C.c_uint32),
                 ("begin_lo", C.c_uint64), ("begin_hi", C.c_uint64),
-                ("end_lo", C.c_uint64), ("end_hi", C.c_uint64)]
+                ("end_lo", C.c_uint64), ("end_hi", C.c_uint64), ("share", C.POINTER(SatShare))]
 
 
 class SatResult(C.Structure):
@@ -328,9 +334,12 @@ class CircuitHandle:
                                                  C.byref(ops)), "stats")
         return live.value, ops.value
 
-    def sat(self, find_all=True, chunk_bits=0, begin=0, end=0):
+    def sat(self, find_all=True, chunk_bits=0, begin=0, end=0, share=None):
+        """SAT solve over [begin, end) (end 0 = 2^n).  share: a SatShare
+        given to every context that takes part in one find-mode search (each
+        in its own thread); the result then covers this context's chunks."""
         o = SatOpts(1 if find_all else 0, chunk_bits, begin & 0xFFFFFFFFFFFFFFFF, begin >> 64,
-                    end & 0xFFFFFFFFFFFFFFFF, end >> 64)
+                    end & 0xFFFFFFFFFFFFFFFF, end >> 64, C.pointer(share) if share is not None else None)
         r = SatResult()
         self.ctx._check(lib().nsat_sat_solve(self.ctx.h, self.h, C.byref(o), C.byref(r)), "sat_solve")
         return {"satisfiable": bool(r.satisfiable), "count": r.count_lo | (r.count_hi << 64),

@@ -39,10 +39,11 @@ int main(int argc, char** argv) {
     }
     ExecType et = parse_exec_type(a.get("exec-type"));
     printf("Execute in %s\n", et.label.c_str());
-    // split over a power-of-two number of devices
-    size_t D = 1;
-    while (D * 2 <= et.devices.size() && (uint32_t)__builtin_ctzll(D * 2) < n) D *= 2;
-    const u128 total = (u128)1 << n;
+    // every device claims launches from one shared queue over the whole
+    // range and stops once any of them holds a witness below its next claim
+    // (the reference's ParSeq mapper, main.rs:205-264)
+    const size_t D = et.devices.size();
+    nsat_sat_share share{};
     std::vector<nsat_sat_result> res(D);
     std::vector<int> rcs(D, 0);
     std::vector<std::string> errs(D);
@@ -60,10 +61,7 @@ int main(int argc, char** argv) {
                 nsat_sat_opts o{};
                 o.find_all = 0;
                 o.chunk_bits = chunk_bits;
-                const u128 b = total / D * i, e = total / D * (i + 1);
-                o.begin_lo = (uint64_t)b; o.begin_hi = (uint64_t)(b >> 64);
-                o.end_lo = (uint64_t)e; o.end_hi = (uint64_t)(e >> 64);
-                if (i + 1 == D && n == 128) { o.end_lo = 0; o.end_hi = 0; }
+                o.share = D > 1 ? &share : nullptr;
                 rc = nsat_sat_solve(ctx, c, &o, &res[i]);
             }
             rcs[i] = rc;
@@ -78,8 +76,12 @@ int main(int argc, char** argv) {
     printf("Time: %.6f\n", now_s() - t0);
     bool found = false;
     u128 w = 0;
-    for (size_t i = 0; i < D && !found; i++)
-        if (res[i].satisfiable) { found = true; w = ((u128)res[i].witness_hi << 64) | res[i].witness_lo; }
+    for (size_t i = 0; i < D; i++) {
+        if (!res[i].satisfiable) continue;
+        const u128 wi = ((u128)res[i].witness_hi << 64) | res[i].witness_lo;
+        if (!found || wi < w) w = wi;
+        found = true;
+    }
     if (found) {
         std::vector<uint8_t> in(n);
         for (uint32_t b = 0; b < n; b++) in[b] = (uint8_t)((w >> b) & 1);

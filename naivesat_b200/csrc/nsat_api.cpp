@@ -267,14 +267,23 @@ uint64_t reverse_bits(uint64_t v, uint32_t bits) {
 // `issue(k, slot)` enqueues launch k, `consume(k, out, ms)` sees its result and
 // returns false to stop issuing.  Device time is the sum of the per-launch
 // CUDA event intervals.
-template <typename Issue, typename Consume>
+// `claim(k, slot)`, when given, is asked before launch k is prepared and
+// returns false when there is nothing more to issue (a shared chunk queue ran
+// out); launches already issued are still consumed.
+struct ClaimAll {
+    bool operator()(uint64_t, int) const { return true; }
+};
+
+template <typename Issue, typename Consume, typename Claim = ClaimAll>
 int run_ring(nsat_ctx* ctx, uint64_t total, Issue issue, Consume consume, double* dev_ms,
-             uint32_t* launches) {
+             uint32_t* launches, Claim claim = Claim()) {
     uint64_t issued = 0, done = 0;
     bool stop = false;
     *dev_ms = 0;
     *launches = 0;
     while (done < issued || (!stop && issued < total)) {
+        if (!stop && issued < total && issued - done < (uint64_t)kRing && !claim(issued, (int)(issued % kRing)))
+            stop = true;
         if (!stop && issued < total && issued - done < (uint64_t)kRing) {
             const int slot = (int)(issued % kRing);
             CK(cudaMemcpyAsync(ctx->d_out + slot, ctx->h_init, sizeof(LaunchOut), cudaMemcpyHostToDevice,
@@ -626,25 +635,47 @@ extern "C" int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opt
     double dev_ms = 0;
     uint32_t launches = 0;
     uint64_t launch_idx_buf[kRing];
+    uint64_t chunk_of_slot[kRing];
     LaunchOut* d_out = ctx->d_out;
+    nsat_sat_share* share = o.find_all ? nullptr : o.share;
     int rc = run_ring(
         ctx, nl,
         [&](uint64_t k, int slot) {
-            launch_idx_buf[slot] = L0 + k;
+            launch_idx_buf[slot] = L0 + (share ? chunk_of_slot[slot] : k);
             LaunchOut* po = d_out + slot;
             void* params[] = {&launch_idx_buf[slot], &po};
             return launch(ctx, fn, grid, threads, params);
         },
         [&](uint64_t k, const LaunchOut& r) {
-            consumed = k + 1;
+            const uint64_t chunk = share ? chunk_of_slot[k % kRing] : k;
+            consumed++;
             count += r.count;
-            if (r.min_idx != ~0ull && !found) {
+            if (r.min_idx != ~0ull) {
+                const u128 w = (((u128)(L0 + chunk)) << C) + r.min_idx;
+                if (!found || w < witness) witness = w;
                 found = true;
-                witness = (((u128)(L0 + k)) << C) + r.min_idx;
+                if (share) {
+                    // no participant claims this chunk or a later one any more
+                    uint64_t cur = __atomic_load_n(&share->stop_plus1, __ATOMIC_ACQUIRE);
+                    while ((cur == 0 || chunk + 1 < cur) &&
+                           !__atomic_compare_exchange_n(&share->stop_plus1, &cur, chunk + 1, false, __ATOMIC_ACQ_REL,
+                                                        __ATOMIC_ACQUIRE)) {
+                    }
+                }
             }
-            return !(found && !o.find_all);
+            // with a shared queue every issued chunk is consumed: a lower
+            // one in flight may hold a lower witness
+            return share ? true : !(found && !o.find_all);
         },
-        &dev_ms, &launches);
+        &dev_ms, &launches,
+        [&](uint64_t, int slot) {
+            if (!share) return true;
+            const uint64_t c = __atomic_fetch_add(&share->next, 1, __ATOMIC_ACQ_REL);
+            const uint64_t st = __atomic_load_n(&share->stop_plus1, __ATOMIC_ACQUIRE);
+            if (c >= nl || (st != 0 && c + 1 >= st)) return false;
+            chunk_of_slot[slot] = c;
+            return true;
+        });
     if (rc) return rc;
     res->satisfiable = found ? 1 : 0;
     const u128 cnt = count >> d;

@@ -141,6 +141,45 @@ __device__ __forceinline__ u32 lut_mux(u32 a, u32 b, u32 c, const Lut& t) {
     return mux(a, mux(b, x67, x45), mux(b, x23, x01));
 }
 
+#ifdef SRV_DISPATCH
+// The truth table of a record as an 8-bit number: bit k of tt is the sign
+// bit of byte k of {thi, tlo}.  (x >> 7) has those bits at 0, 8, 16, 24, and
+// the product with 0x01020408 gathers them into bits 24..27 (every other
+// partial product lands below bit 24 at a distinct position, or above bit
+// 31), so the gather is two shifts and a multiply per word.
+__device__ __forceinline__ u32 tt_of(u32 tlo, u32 thi) {
+    const u32 lo = ((tlo >> 7) * 0x01020408u) >> 24;
+    const u32 hi = ((thi >> 7) * 0x01020408u) >> 24;
+    return lo | (hi << 4);
+}
+
+// One LUT on W words with its truth table as the lop3 immediate: the table
+// is the same for the whole warp (every lane runs the same program), so the
+// switch is a uniform jump and each word costs one lop3.
+template <int T>
+__device__ __forceinline__ void lut_imm(const Vals& a, const Vals& b, const Vals& c, Vals& d) {
+#pragma unroll
+    for (int w = 0; w < W; w++) d.v[w] = lop3<T>(a.v[w], b.v[w], c.v[w]);
+}
+
+#define SRV_CASE(t) \
+    case (t): lut_imm<(t)>(a, b, c, d); break;
+#define SRV_CASE4(t) SRV_CASE(t) SRV_CASE((t) + 1) SRV_CASE((t) + 2) SRV_CASE((t) + 3)
+#define SRV_CASE16(t) SRV_CASE4(t) SRV_CASE4((t) + 4) SRV_CASE4((t) + 8) SRV_CASE4((t) + 12)
+#define SRV_CASE64(t) SRV_CASE16(t) SRV_CASE16((t) + 16) SRV_CASE16((t) + 32) SRV_CASE16((t) + 48)
+
+__device__ __forceinline__ Vals lut_switch(u32 tt, const Vals& a, const Vals& b, const Vals& c) {
+    Vals d;
+    switch (tt & 255u) {
+        SRV_CASE64(0)
+        SRV_CASE64(64)
+        SRV_CASE64(128)
+        SRV_CASE64(192)
+    }
+    return d;
+}
+#endif
+
 // Slot fields decoded with multiply-adds (FMA pipe) instead of masks and
 // shifts (ALU pipe, the kernel's bound): hi = x * km >> 32 with km = 65536,
 // lo = x - hi * km, byte offset = field * sb; km and sb come from the epoch
@@ -179,10 +218,14 @@ __device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32
         for (int k = 0; k < G; k++) nxt[k] = __ldg(nx + k);
 #pragma unroll
         for (int k = 0; k < G; k++) {
+#ifdef SRV_DISPATCH
+            const Vals d = lut_switch(tt_of(cur[k].z, cur[k].w), a[k], b[k], c[k]);
+#else
             const Lut t = expand(cur[k]);
             Vals d;
 #pragma unroll
             for (int w = 0; w < W; w++) d.v[w] = lut_mux(a[k].v[w], b[k].v[w], c[k].v[w], t);
+#endif
             sts(Sl + dof[k], d);
         }
 #pragma unroll

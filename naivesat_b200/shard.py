@@ -1,8 +1,11 @@
 """Multi-GPU sharding of the SAT and QSAT searches: one process per GPU,
 no data-path collective, one small exchange of per-rank answers.
 
-- SAT: rank r scans the contiguous index range [r*2^n/W, (r+1)*2^n/W); the
-  ranks' (count, lowest witness) are combined by sum and min.
+- SAT, count mode: rank r scans the contiguous index range
+  [r*2^n/W, (r+1)*2^n/W); the ranks' (count, lowest witness) are combined
+  by sum and min.
+- SAT, find mode: chunks are dealt round-robin and the ranks exchange their
+  lowest witness after every round, so all of them stop once any has one.
 - QSAT: rank r fixes the outermost log2(W) inputs to r (input 0 most
   significant) and solves the sub-formula below them
   (nsat_qsat_opts.prefix_bits/prefix); the W sub-answers, in rank order, are
@@ -127,6 +130,34 @@ def sharded_sat(solve_range, n, world, rank):
     begin, end = shard_range(1 << n, world, rank)
     mine = solve_range(begin, end)
     return combine_sat(exchange({"count": mine["count"], "witness": mine["witness"]}, world))
+
+
+def sharded_sat_find(solve_range, n, world, rank, chunk_bits):
+    """Find mode (the lowest witness) with a stop shared by every rank, the
+    arrangement of the reference's ParSeq mapper, which hands args to the
+    free device and stops all of them once one has a witness (main.rs:205-264).
+    The index space is cut into chunks of 2^chunk_bits; in round t rank r
+    scans chunk t*world + r, so the ranks move through the space together;
+    after each round the ranks exchange their lowest witness, and they all
+    stop once one exists: every chunk below it was scanned in that round or
+    earlier.  solve_range(begin, end) -> {witness, count} (find mode: the
+    count covers what the solver scanned).  Returns the answer on every rank
+    with this rank's share of the work (scanned assignments, rounds)."""
+    cb = min(chunk_bits, n)
+    nchunks = 1 << (n - cb)
+    mine, count, scanned, t = None, 0, 0, 0
+    while True:
+        c = t * world + rank
+        if c < nchunks and mine is None:
+            r = solve_range(c << cb, (c + 1) << cb)
+            count += r["count"]
+            scanned += 1 << cb
+            mine = r["witness"]
+        t += 1
+        lows = [w for w in exchange(mine, world) if w is not None]
+        if lows or t * world >= nchunks:
+            return {"satisfiable": bool(lows), "witness": min(lows) if lows else None,
+                    "scanned": scanned, "rounds": t, "count_scanned": count}
 
 
 def sharded_qsat(solve_prefix, quants, world, rank):

@@ -1,6 +1,19 @@
 """QSAT results pinned by the reference's
 test_opencl_quant_reducer_final_result_with_circuit (qsat.rs:6033-6267).
 
+All twelve vectors run here.  The reference test hands its reducer an
+already-decided prefix (the first `solution_bits` inputs, with its
+FinalResult) and checks final_result_with_circuit (qsat.rs:1266-1320): when
+the first quantifier block continues below the prefix and the prefix has a
+solution, the reducer evaluates the circuit over the remaining inputs and
+joins the tail's FinalResult to the prefix's (FinalResult::join,
+qsat.rs:109-133); otherwise it passes the prefix's result through.  Here the
+tail is the sub-formula below a fixed prefix, solved through
+nsat_qsat_opts.prefix_bits/prefix on the GPU and by the oracle on the CPU,
+then joined the same way.  Five vectors (5, 8, 9, 10, 11) are pass-through:
+the first block ends with the prefix, or the prefix carries no solution, so
+no circuit is evaluated and the expected result is the prefix's own.
+
 Its circuits are specified by gen_circuit (qsat.rs:6010-6030): with sb
 "solution bits" and 5 table bits,
     f(x) = T[x_sb .. x_sb+4] AND (x_0 .. x_sb-1 == solution),
@@ -97,3 +110,70 @@ def test_gpu_reproduces_reference_results(ctx):
         circ = lookup_circuit(c["circuit_solution_bits"], c["solution"], c["values"])
         r = ctx.circuit(circ).qsat(c["quants"])
         assert {k: r[k] for k in ("reversed", "solution_bits", "solution")} == c["expected"], i
+
+
+def first_block_len(q):
+    return len(q) - len(q.lstrip(q[0]))
+
+
+def join(a, b):
+    """FinalResult::join (qsat.rs:109-133)."""
+    assert a["reversed"] == b["reversed"]
+    bits = a["solution_bits"] + b["solution_bits"]
+    if a["solution"] is None:
+        assert b["solution"] is None
+        return {"reversed": a["reversed"], "solution_bits": bits, "solution": None}
+    assert b["solution"] is not None
+    return {"reversed": a["reversed"], "solution_bits": bits,
+            "solution": (a["solution"] | (b["solution"] << a["solution_bits"])) & ((1 << bits) - 1)}
+
+
+def prefix_value(solution, sb):
+    """nsat's prefix (input 0 most significant) of a FinalResult solution
+    (bit k = input k)."""
+    return int(format(solution, "0%db" % sb)[::-1], 2)
+
+
+def with_prefix(c, solve_sub):
+    """The reducer's final_result_with_circuit restated over a sub-formula
+    solver: returns (expected-comparable result, evaluated a circuit?)."""
+    sb, q = c["circuit_solution_bits"], c["quants"]
+    head = {"reversed": q[0] == "A", "solution_bits": sb,
+            "solution": c["solution"] if c["expected"]["solution"] is not None else None}
+    if first_block_len(q) <= sb or head["solution"] is None:
+        return head, False
+    sub = solve_sub(sb, prefix_value(c["solution"], sb))
+    tail = {k: sub[k] for k in ("reversed", "solution_bits", "solution")}
+    return join(head, tail), True
+
+
+def all_cases():
+    return json.load(open(os.path.join(HERE, "golden", "final_result_circuit.json")))["cases"]
+
+
+def test_every_vector_through_prefix_subproblems_on_the_oracle():
+    from test_shard import fix_prefix
+    evaluated = []
+    for i, c in enumerate(all_cases()):
+        circ = lookup_circuit(c["circuit_solution_bits"], c["solution"], c["values"])
+
+        def solve_sub(s, p):
+            return O.qsat(fix_prefix(circ, s, p), c["quants"][s:], mode=1)
+        got, ev = with_prefix(c, solve_sub)
+        assert got == c["expected"], (i, got, c["expected"])
+        if ev:
+            evaluated.append(i)
+    assert evaluated == [0, 1, 2, 3, 4, 6, 7]
+
+
+@pytest.mark.gpu
+def test_every_vector_through_prefix_subproblems_on_gpu(ctx):
+    evaluated = []
+    for i, c in enumerate(all_cases()):
+        circ = lookup_circuit(c["circuit_solution_bits"], c["solution"], c["values"])
+        h = ctx.circuit(circ)
+        got, ev = with_prefix(c, lambda s, p: h.qsat(c["quants"], prefix_bits=s, prefix=p))
+        assert got == c["expected"], (i, got, c["expected"])
+        if ev:
+            evaluated.append(i)
+    assert evaluated == [0, 1, 2, 3, 4, 6, 7]

@@ -53,3 +53,45 @@ def test_sharded_qsat_adder_known_answer(ctx):
     subs = [h.qsat(b.quants, prefix_bits=2, prefix=p) for p in range(4)]
     comb = shard.combine_qsat(b.quants, subs)
     assert comb["value"] is False and comb["solution"] == 0 and comb["solution_bits"] == 16
+
+
+def _solve_shared(ctx0, ctx1, circ, chunk_bits):
+    """One find-mode search split over two contexts on the same GPU, each
+    on its own host thread, through one nsat_sat_share queue."""
+    import threading
+    from naivesat_b200 import api
+    share = api.SatShare()
+    hs = [ctx0.circuit(circ), ctx1.circuit(circ)]
+    out = [None, None]
+
+    def run(i):
+        out[i] = hs[i].sat(find_all=False, chunk_bits=chunk_bits, share=share)
+    th = [threading.Thread(target=run, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    lows = [r["witness"] for r in out if r["witness"] is not None]
+    return (min(lows) if lows else None), out
+
+
+def test_shared_queue_two_contexts_stop_together(ctx):
+    """Two contexts claim launches from one shared queue: with an early
+    witness both stop within a few launches of it (not after half the index
+    space each); the lowest witness equals the single-context solve's; with
+    no solution the two together scan every chunk exactly once."""
+    from naivesat_b200 import api
+    with api.Context(0) as other:
+        early = W.Circuit(30, [(W.AND, 0, 2)], [(30, 0)], name="x0 and x2")
+        low, out = _solve_shared(ctx, other, early, 20)
+        assert low == 5
+        # each context has at most a ring of launches in flight when the stop lands
+        assert all(r["scanned"] <= 16 << 20 for r in out), [r["scanned"] for r in out]
+        for seed in range(4):
+            c = W.random_dag(1200 + seed, 26, 400, output="live")
+            one = ctx.circuit(c).sat(find_all=False, chunk_bits=18)
+            low, out = _solve_shared(ctx, other, c, 18)
+            assert low == one["witness"], (seed, low, one["witness"])
+        unsat = W.Circuit(24, [(W.NIMPL, 3, 3)], [(24, 0)], name="contradiction")
+        low, out = _solve_shared(ctx, other, unsat, 18)
+        assert low is None and sum(r["scanned"] for r in out) == 1 << 24

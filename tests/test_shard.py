@@ -122,3 +122,52 @@ def test_two_rank_gloo_exchange(tmp_path):
             got = json.load(f)
         assert (got["sat"]["count"], got["sat"]["witness"]) == (cnt, low)
         assert {k: got["qsat"][k] for k in full} == full
+
+
+def _find_rank_main(rank, world, port, outdir):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        out = {}
+        for name, c in find_cases():
+            oc = O.Circuit(c.n, c.gates, c.outputs)
+
+            def solve(b, e):
+                k, w = O.sat_range(oc, b, e, 2)
+                return {"count": k, "witness": w}
+            out[name] = shard.sharded_sat_find(solve, c.n, world, rank, 12)
+        with open(os.path.join(outdir, "find%d.json" % rank), "w") as f:
+            json.dump(out, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def find_cases():
+    return [("early", W.Circuit(18, [(W.AND, 0, 2)], [(18, 0)], name="x0 and x2")),
+            ("random", W.random_dag(33, 18, 300, output="live")),
+            ("unsat", W.Circuit(18, [(W.NIMPL, 3, 3)], [(18, 0)], name="contradiction"))]
+
+
+def test_two_rank_find_mode_stops_every_rank(tmp_path):
+    """Find mode over 2 gloo ranks: with the lowest witness in rank 0's first
+    chunk both ranks stop after one round (rank 1 scans one chunk, not its
+    half of the space); answers equal the oracle's lowest witness; with no
+    solution every chunk is scanned once."""
+    world = 2
+    mp.start_processes(_find_rank_main, args=(world, free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    got = []
+    for r in range(world):
+        with open(tmp_path / ("find%d.json" % r)) as f:
+            got.append(json.load(f))
+    for name, c in find_cases():
+        cnt, low = O.sat_range(O.Circuit(c.n, c.gates, c.outputs))
+        for r in range(world):
+            assert (got[r][name]["satisfiable"], got[r][name]["witness"]) == (low is not None, low), (name, r)
+        if name == "early":
+            assert low == 5
+            assert all(got[r][name]["rounds"] == 1 and got[r][name]["scanned"] == 1 << 12 for r in range(world))
+        if name == "unsat":
+            assert sum(got[r][name]["scanned"] for r in range(world)) == 1 << 18
