@@ -15,6 +15,9 @@ literals and the test helpers `str_to_quants`/`str_to_bools`) and writes:
   aggr_tree_cpu.json        qsat.rs:2629-2835  test_aggr_output_cpu_code
   aggr_tree_opencl.json     qsat.rs:3434-3520  test_aggr_output_opencl_code
   final_result_circuit.json qsat.rs:6033-6267  final_result_with_circuit
+  opencl_quant_reducer.json qsat.rs:4038-6008  test_opencl_quant_reducer
+  cpu_outputs_final_result.json qsat.rs:3859-4036
+                            test_get_final_results_from_cpu_outputs
   greedy_find_solution.json greedysatostop.rs:1204-1268
   greedy_mem_image.json     greedysatostop.rs:1145-1201
   greedy_file_image.json    greedysatostop.rs:1271-1354
@@ -35,7 +38,7 @@ TOKEN_RE = re.compile(
         (?P<str>"(?:[^"\\]|\\.)*")
       | (?P<num>0x[0-9a-fA-F_]+|0b[01_]+|[0-9][0-9_]*)(?P<suf>u8|u16|u32|u64|u128|usize|i32|i64)?
       | (?P<id>[A-Za-z_][A-Za-z0-9_]*)
-      | (?P<op>::|\.\.|<<|>>|=>|[()\[\]{},;:&|+\-*.!<>_?=])
+      | (?P<op>::|\.\.|<<|>>|=>|==|!=|[()\[\]{},;:&|+\-*.!<>_?=])
     )""",
     re.VERBOSE,
 )
@@ -72,12 +75,17 @@ def tokenize(src):
     return toks
 
 
+class Repeat:
+    def __init__(self, value):
+        self.value = value
+
+
 class Closure:
-    def __init__(self, param, body, parser):
-        self.param, self.body, self.parser = param, body, parser
+    def __init__(self, param, body, parser, env=None):
+        self.param, self.body, self.parser, self.env = param, body, parser, dict(env or {})
 
     def __call__(self, x):
-        return self.parser.eval_ast(self.body, {self.param: x})
+        return self.parser.eval_ast(self.body, dict(self.env, **{self.param: x}))
 
 
 def str_to_quants(s):
@@ -91,7 +99,7 @@ def str_to_bools(s):
 class Parser:
     """Builds a tiny AST and evaluates it; binary precedence follows Rust."""
 
-    PREC = [("|",), ("^",), ("&",), ("<<", ">>"), ("+", "-"), ("*",)]
+    PREC = [("==", "!="), ("|",), ("^",), ("&",), ("<<", ">>"), ("+", "-"), ("*",)]
 
     def __init__(self, src):
         self.t = tokenize(src)
@@ -134,7 +142,11 @@ class Parser:
         if self.is_op("-"):
             self.take()
             return ("neg", self.unary())
-        return self.postfix(self.primary())
+        node = self.postfix(self.primary())
+        while self.peek() == ("id", "as"):       # `as u16`: truncation to the type
+            self.take()
+            node = ("cast", self.take("id")[1], node)
+        return node
 
     def postfix(self, node):
         while self.is_op("."):
@@ -172,6 +184,13 @@ class Parser:
             self.take("op", "|")
             return ("closure", param, self.expr())
         return self.expr()
+
+    def block(self):
+        """`{ expr }`: a block whose value is its one expression."""
+        self.take("op", "{")
+        e = self.expr()
+        self.take("op", "}")
+        return e
 
     def seq(self, close):
         items = []
@@ -215,6 +234,15 @@ class Parser:
         if self.is_op("["):
             self.take()
             return self.seq("]")
+        if self.is_op("{"):
+            return self.block()
+        if tok == ("id", "if"):
+            self.take()
+            cond = self.expr()
+            then = self.block()
+            self.take("id", "else")
+            other = self.block() if self.is_op("{") else self.primary()
+            return ("if", cond, then, other)
         if tok[0] == "id":
             name = self.take()[1]
             # path segments: Option::<FinalResult>::None, std::iter::...
@@ -283,9 +311,15 @@ class Parser:
             return env.get(n[1], n[1])
         if k == "neg":
             return -self.eval_ast(n[1], env)
+        if k == "if":
+            return self.eval_ast(n[2] if self.eval_ast(n[1], env) else n[3], env)
+        if k == "cast":
+            bits = {"u8": 8, "u16": 16, "u32": 32, "u64": 64, "u128": 128, "usize": 64}[n[1]]
+            return self.eval_ast(n[2], env) & ((1 << bits) - 1)
         if k == "bin":
             a, b = self.eval_ast(n[2], env), self.eval_ast(n[3], env)
-            return {"|": lambda: a | b, "^": lambda: a ^ b, "&": lambda: a & b,
+            return {"==": lambda: a == b, "!=": lambda: a != b,
+                    "|": lambda: a | b, "^": lambda: a ^ b, "&": lambda: a & b,
                     "<<": lambda: a << b, ">>": lambda: a >> b, "+": lambda: a + b,
                     "-": lambda: a - b, "*": lambda: a * b}[n[1]]()
         if k == "range":
@@ -297,7 +331,7 @@ class Parser:
         if k == "repeat":
             return [self.eval_ast(n[1], env)] * self.eval_ast(n[2], env)
         if k == "closure":
-            return Closure(n[1], n[2], self)
+            return Closure(n[1], n[2], self, env)
         if k == "struct":
             return dict(_type=n[1], **{f: self.eval_ast(v, env) for f, v in n[2].items()})
         if k == "call":
@@ -311,6 +345,10 @@ class Parser:
                 return "".join(args)
             if name == "Some":
                 return args[0]
+            if name == "repeat":          # iter::repeat(x): unbounded until .take(n)
+                return Repeat(args[0])
+            if name == "once":            # iter::once(x)
+                return [args[0]]
             raise ValueError("unknown call " + name)
         if k == "method":
             name, base = n[1], self.eval_ast(n[2], env)
@@ -321,8 +359,25 @@ class Parser:
                 return list(base) + list(args[0])
             if name == "map":
                 return [args[0](x) for x in base]
+            if name == "flatten":
+                return [x for part in base for x in part]
+            if name == "rotate_left":         # the tests rotate u64 literals
+                r = args[0] % 64
+                return ((base << r) | (base >> (64 - r))) & ((1 << 64) - 1)
+            if name == "take":
+                return [base.value] * args[0] if isinstance(base, Repeat) else list(base)[:args[0]]
             raise ValueError("unknown method " + name)
         raise ValueError("bad node %r" % (k,))
+
+
+def rle(values):
+    out = []
+    for v in values:
+        if out and out[-1][0] == v:
+            out[-1][1] += 1
+        else:
+            out.append([v, 1])
+    return out
 
 
 def fn_body(src, name):
@@ -417,6 +472,48 @@ def main():
         "note": "circuit = booltable(inputs[sb..sb+5], values) AND inputs[0..sb]==solution "
                 "(gen_circuit, qsat.rs:6010-6030); the expected value completes the first-"
                 "quantifier bits below sb from the circuit with inputs[0..sb] fixed",
+        "cases": cases}
+
+    body, line = fn_body(qsat, "test_opencl_quant_reducer")
+    cases = []
+    for k, (rsb, reb, iglb, quants, group_len, tests) in enumerate(parse_cases(body)):
+        for (inputs, (exp, value)) in tests:
+            cases.append({"case": k, "reduce_start_bit": rsb, "reduce_end_bit": reb, "init_group_len_bits": iglb,
+                          "quants": quants, "group_len": group_len, "inputs_rle": rle(inputs),
+                          "expected": None if exp is None else final_result(exp), "value": bool(value)})
+    out["opencl_quant_reducer.json"] = {
+        "source": "src/qsat.rs:%d test_opencl_quant_reducer" % line,
+        "note": "inputs: one u16 per group of the bits reduce_end_bit..reduce_end_bit+init_group_len_bits "
+                "(bit 15 the group's value, bits 0..14 the group-local index of the first decisive unit, "
+                "0x7fff none), groups in index order over bits reduce_start_bit..reduce_end_bit, stored as "
+                "[value, run length] pairs; expected: "
+                "the reducer's FinalResult (None when it has none) and the formula's value",
+        "cases": cases}
+
+    body, line = fn_body(qsat, "test_get_final_results_from_cpu_outputs")
+    cases = []
+    for m in re.finditer(r"assert_eq!\(", body):
+        i, depth = m.end() - 1, 0
+        for j in range(i, len(body)):
+            depth += {"(": 1, ")": -1}.get(body[j], 0)
+            if depth == 0:
+                break
+        call = body[i + 1:j]
+        k = call.index("get_final_results_from_cpu_outputs(")
+        exp, value = Parser(call[:k].rstrip().rstrip(",")).eval_ast(Parser(call[:k].rstrip().rstrip(",")).primary())
+        args = call[k + len("get_final_results_from_cpu_outputs("):]
+        type_len, elem_bits = (int(x) for x in re.findall(r"\d+", args)[:2])
+        quants = str_to_quants(re.search(r'str_to_quants\("([^"]*)"\)', args).group(1))
+        arr = args[args.index("&[") + 1:args.rindex("[..]")]
+        p2 = Parser(arr)
+        outputs = p2.eval_ast(p2.primary())
+        cases.append({"type_len": type_len, "elem_bits": elem_bits, "quants": quants, "outputs": outputs,
+                      "expected": None if exp is None else final_result(exp), "value": bool(value)})
+    out["cpu_outputs_final_result.json"] = {
+        "source": "src/qsat.rs:%d test_get_final_results_from_cpu_outputs" % line,
+        "note": "outputs: words 0..type_len/32 the lane values of the deciding word, then the call's value, "
+                "a solution flag and the deciding word's index (low, high) within the call; expected: the "
+                "FinalResult of the call's part of the formula (None when it has none) and the call's value",
         "cases": cases}
 
     body, line = fn_body(greedy, "test_mem_image_find_solution")
