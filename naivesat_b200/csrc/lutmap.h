@@ -2,9 +2,11 @@
 //
 // A 3-input LUT is exactly what one lop3.b32 instruction computes, so the
 // number of LUTs is the number of logic instructions per 32-lane word.  The
-// mapper enumerates cuts of at most 3 leaves per node, picks cuts by area flow
-// (Cong & Ding style priority cuts), then does exact-area recovery passes.
-// Negations never cost an instruction: they live in the truth tables.
+// mapper enumerates cuts with their truth tables, reduces each to the support
+// of its function, picks 3-leaf cuts by area flow (Cong & Ding style priority
+// cuts), then does exact-area recovery passes.  Negations never cost an
+// instruction: they live in the truth tables.  A node whose function is
+// constant becomes a LUT with a constant table that reads input 0.
 #pragma once
 #include <cstdint>
 #include <vector>
@@ -15,7 +17,7 @@ namespace nsat {
 
 struct Lut {
     uint32_t wire;       // circuit wire this LUT computes
-    uint8_t nin;         // 1..3 leaves
+    uint8_t nin;         // 1..3 leaves (a constant LUT has 1, input 0, ignored)
     uint32_t in[3];      // leaf wires (operands a, b, c of lop3)
     uint8_t tt;          // lop3 immediate: f(a,b,c) = bit (a<<2 | b<<1 | c)
 };
@@ -29,7 +31,13 @@ struct LutNet {
 
 // Maps the cone of outputs `which` (indices into c.outputs).  With
 // one_per_gate, every live gate becomes its own 2-leaf LUT (no fusion).
-LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate);
+// cut_leaves (3..6) bounds the cuts enumerated before support reduction:
+// wider finds smaller covers and costs more time (3000 gates: about 2, 10
+// and 35 ms at 3, 4 and 6).
+constexpr int kCutLeavesCompiled = 6;   // compiled kernels: NVRTC costs far more than mapping
+constexpr int kCutLeavesServed = 4;     // serving programs: mapped per request on builder threads
+LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate,
+                int cut_leaves = kCutLeavesCompiled);
 
 // Reference evaluation of a LutNet on 32-lane words (used by host self-checks).
 void eval_lutnet32(const LutNet& net, uint32_t nwires, const uint32_t* inputs, uint32_t* outs);

@@ -108,7 +108,7 @@ struct Program {
 };
 
 bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool raw, Program* p, std::string* err) {
-    LutNet net = map_luts(c, which, raw);
+    LutNet net = map_luts(c, which, raw, kCutLeavesServed);
     const uint32_t W = c.wires();
     const size_t L = net.luts.size();
     std::vector<int32_t> lut_of(W, -1);
