@@ -696,6 +696,11 @@ def run_serving_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def sm_count(device):
+    import torch
+    return torch.cuda.get_device_properties(device).multi_processor_count
+
+
 def run_serving(args, world, rank, local):
     """Config 4: 10,000 SAT/QSAT/SATOSTOP requests (70/20/10) with Poisson
     arrivals through the batched server, against the plain one-launch-per-
@@ -706,7 +711,10 @@ def run_serving(args, world, rank, local):
     ctx = api.Context(local)
     reqs = W.serving_requests(args.requests, seed=2024, rate_hz=args.rate)
     warm = W.serving_requests(64, seed=99, rate_hz=1e9)
-    srv_kw = dict(epoch_budget=48000000)
+    # the interpreter's shape and epoch budget for this GPU (persisted in the
+    # kernel cache; servers created with the defaults use them)
+    tune = api.server_tune(ctx, persist=True, retune=True)
+    srv_kw = dict()
 
     peak_lop3, probe_mhz = ctx.lop3_peak()
     srv = api.Server(ctx, **srv_kw)
@@ -794,10 +802,14 @@ def run_serving(args, world, rank, local):
                for i in pres_low)
     plain_low_lat = serving.fifo_latencies([r["arrival_s"] for r in low], svc_low)
 
-    # interpreter work: tiles x program length (NOPs included) x 1024 words per tile
-    ins = [sum(api.server_program_check(r["circ"], r["kind"])[1:]) for r in reqs]
-    words = sum(res_sat[i]["tiles"] * 1024 * ins[i] for i in res_sat)
+    # interpreter work: tiles x LUTs x 1024 words per tile (padding NOPs not counted)
+    shape = st_sat["shape"]
+    luts = [api.server_program_check(r["circ"], r["kind"], shape=shape)[1] for r in reqs]
+    words = sum(res_sat[i]["tiles"] * 1024 * luts[i] for i in res_sat)
     lut_words = words / (st_sat["device_ms"] * 1e-3)
+    # every LUT-word reads three slot words and writes one in shared memory:
+    # 16 bytes against 128 bytes per SM clock
+    smem_peak = sm_count(local) * 128 * probe_mhz * 1e6 / 1e9
     cpu = None
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -826,12 +838,14 @@ def run_serving(args, world, rank, local):
         "low_rate": {"rate_hz": args.low_rate, "requests": len(low),
                      "server": serving.summarize(lat_low, mk_low, len(res_low)),
                      "plain": serving.summarize(plain_low_lat, sum(svc_low), len(svc_low))},
-        "roofline": {"bound": "alu", "kernel": "serve_epoch",
-                     "achieved": 7 * lut_words, "peak": peak_lop3, "unit": "lop3/s",
-                     "frac": 7 * lut_words / peak_lop3, "traffic": None,
-                     "lut_words_per_s": lut_words,
-                     "note": "a run-time LUT costs 7 lop3 (mux tree over truth-table masks) per 32-bit word",
-                     "peak_source": "measured lop3.b32 chain microbenchmark on this GPU (%.0f MHz)" % probe_mhz},
+        "roofline": {"bound": "smem", "kernel": "serve_epoch",
+                     "achieved": lut_words * 16 / 1e9, "peak": smem_peak, "unit": "GB/s",
+                     "frac": lut_words * 16 / 1e9 / smem_peak, "traffic": None,
+                     "lut_words_per_s": lut_words, "lop3_issue_frac": lut_words / peak_lop3,
+                     "note": "each LUT-word reads 3 and writes 1 slot word of shared memory (16 B); peak = SMs x "
+                             "128 B/clk x the SM clock the lop3 probe measured",
+                     "peak_source": "architectural shared-memory width x measured clock (%.0f MHz)" % probe_mhz},
+        "interpreter_tuning": dict(tune, shape_used=shape),
         "cpu_baseline": cpu,
         "e2e": {"value": sat_sum["solves_per_s"], "unit": "solves/s",
                 "h2d_bytes_per_step": st_sat["h2d_bytes"] / len(reqs),

@@ -325,9 +325,10 @@ typedef struct {
     uint32_t max_queue;         /* waiting jobs before submit returns NSAT_EBUSY; 0 = 2^20 */
     uint32_t max_slice_tiles;   /* cap of one job's tiles per epoch; 0 = 4096 */
     uint32_t first_slice_tiles; /* a new job's first slice (doubling after); 0 = 1 */
-    uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = 4.8e7
-                                   (about 30 ms of device time; on the config-4 trace smaller
-                                   budgets raise p99 and lower solves/s) */
+    uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = the
+                                   budget nsat_server_tune persisted for this GPU, else 4.8e7
+                                   (on the config-4 trace smaller budgets raised p99 and lowered
+                                   solves/s) */
     uint32_t build_threads;     /* host threads that build job programs; 0 = min(8, cores / 2) */
     uint32_t tier_threads;      /* QSAT tiering workers (own context each); 0 = three quarters of
                                    the host threads, between 2 and 12 */
@@ -338,7 +339,19 @@ typedef struct {
                                    0xFFFFFFFF = never */
     uint32_t tier_wait;         /* 1: such a job is not interpreted until its kernel is ready, so
                                    every block runs compiled (compile first instead of racing) */
+    uint32_t shape;             /* interpreter shape, 1..NSAT_SERVE_SHAPES (below); 0 = the shape
+                                   nsat_server_tune persisted for this GPU, else the default */
+    uint32_t reserved;
 } nsat_server_opts;
+
+/* Interpreter shapes: words per lane W (W x 1024 assignments per warp and
+ * program pass), groups of G mutually independent instructions (a group's
+ * operands are loaded before any result is stored), and the evaluation of a
+ * LUT with a run-time truth table, either a 7-lop3 mux tree over masks or a
+ * jump on the warp-uniform table to one lop3 per word:
+ *   1: W4 G4 mux   2: W4 G1 jump   3: W4 G2 jump
+ *   4: W4 G4 jump  5: W2 G1 jump   6: W2 G2 jump */
+#define NSAT_SERVE_SHAPES 6
 
 typedef struct {
     uint32_t kind;              /* 0 = SAT, 1 = QSAT, 2 = SATOSTOP */
@@ -385,7 +398,39 @@ typedef struct {
     uint32_t graph_slots, grid;
     uint64_t launches;          /* kernels launched: epoch graphs and join rounds */
     uint64_t h2d_bytes, d2h_bytes;   /* host<->device copies issued: programs, epoch tables, results */
+    uint32_t shape;             /* the interpreter shape in use (1-based) */
+    uint32_t reserved;
 } nsat_server_stats_t;
+
+/* Autotuner of the batched interpreter (no counterpart in the reference).
+ * Serves a seeded calibration set of SAT jobs in count mode (every tile
+ * evaluated, so the work is fixed: 18-28 inputs, 100-4000 gates) under every
+ * interpreter shape and keeps the one with the most LUT-words per second of
+ * device time; then, for that shape, times the same set with epoch budgets of
+ * 1.2e7 .. 9.6e7 and keeps the one with the best throughput whose mean epoch
+ * stays under 20 ms (longer epochs delay arrivals).  With `persist` the
+ * choice is written to the kernel cache directory, keyed by GPU, and servers
+ * created later with shape 0 and epoch_budget 0 use it; an existing choice is
+ * read back instead of timing again unless `retune` is set. */
+typedef struct {
+    uint32_t jobs;          /* calibration jobs (0 = 24) */
+    uint32_t persist;
+    uint32_t retune;        /* time again even if a persisted choice exists */
+    uint32_t reserved;
+    uint64_t seed;          /* calibration set (0 = the fixed default) */
+} nsat_serve_tune_opts;
+
+typedef struct {
+    uint32_t shape;                                /* chosen, 1-based */
+    uint32_t from_cache;                           /* read back, nothing timed */
+    uint64_t epoch_budget;                         /* chosen */
+    double lut_words_per_s[NSAT_SERVE_SHAPES];     /* per shape, device time (0 = not timed) */
+    double budget_solves_per_s[4];                 /* budgets 1.2e7, 2.4e7, 4.8e7, 9.6e7: wall clock */
+    double budget_epoch_ms[4];                     /* their mean epoch wall time */
+    double tune_ms;
+} nsat_serve_tune_result;
+
+int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts, nsat_serve_tune_result* res);
 
 int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out);
 void nsat_server_destroy(nsat_server* s);
@@ -402,13 +447,14 @@ int nsat_server_step(nsat_server* s, uint32_t* active, uint32_t* queued);
 int nsat_server_poll(nsat_server* s, nsat_job_result* out, uint32_t cap, uint32_t* n);
 int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st);
 
-/* Host-only check of the interpreter program a job of `kind` would get:
- * builds it, runs it on the host with the kernel's group semantics (a
- * group's operands are read before any of its results is written) for two
- * passes of 64 seeded random assignments, and compares every requested
- * output with direct evaluation of the circuit.  Reports the program's
- * slots, LUTs and padding NOPs.  NSAT_EINVAL on a mismatch.  Needs no GPU. */
-int nsat_server_program_check(const nsat_circuit_desc* circuit, uint32_t kind, uint64_t seed,
+/* Host-only check of the interpreter program a job of `kind` would get on a
+ * server of `shape` (1-based; 0 = the default shape): builds it, runs it on
+ * the host with the kernel's group semantics (a group's operands are read
+ * before any of its results is written) for two passes of 64 seeded random
+ * assignments, and compares every requested output with direct evaluation
+ * of the circuit.  Reports the program's slots, LUTs and padding NOPs.
+ * NSAT_EINVAL on a mismatch.  Needs no GPU. */
+int nsat_server_program_check(const nsat_circuit_desc* circuit, uint32_t kind, uint32_t shape, uint64_t seed,
                               uint32_t* slots, uint32_t* luts, uint32_t* nops);
 
 /* ---- seeded benchmark circuits ------------------------------------------- */

@@ -111,7 +111,19 @@ class ServerOpts(C.Structure):
     _fields_ = [("arena_bytes", C.c_uint64), ("max_active", C.c_uint32), ("max_queue", C.c_uint32),
                 ("max_slice_tiles", C.c_uint32), ("first_slice_tiles", C.c_uint32),
                 ("epoch_budget", C.c_uint64), ("build_threads", C.c_uint32), ("tier_threads", C.c_uint32),
-                ("tier_min_ms", C.c_uint32), ("tier_wait", C.c_uint32)]
+                ("tier_min_ms", C.c_uint32), ("tier_wait", C.c_uint32), ("shape", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class ServeTuneOpts(C.Structure):
+    _fields_ = [("jobs", C.c_uint32), ("persist", C.c_uint32), ("retune", C.c_uint32), ("reserved", C.c_uint32),
+                ("seed", C.c_uint64)]
+
+
+class ServeTuneResult(C.Structure):
+    _fields_ = [("shape", C.c_uint32), ("from_cache", C.c_uint32), ("epoch_budget", C.c_uint64),
+                ("lut_words_per_s", C.c_double * 6), ("budget_solves_per_s", C.c_double * 4),
+                ("budget_epoch_ms", C.c_double * 4), ("tune_ms", C.c_double)]
 
 
 class JobDesc(C.Structure):
@@ -135,7 +147,8 @@ class ServerStats(C.Structure):
     _fields_ = [("epochs", C.c_uint64), ("device_ms", C.c_double), ("active", C.c_uint32),
                 ("queued", C.c_uint32), ("arena_used", C.c_uint64), ("arena_bytes", C.c_uint64),
                 ("graph_slots", C.c_uint32), ("grid", C.c_uint32), ("launches", C.c_uint64),
-                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("shape", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 EXPORTS = [
@@ -147,7 +160,7 @@ EXPORTS = [
     "nsat_qsat_solve_noalloc", "nsat_server_create", "nsat_server_destroy", "nsat_server_submit",
     "nsat_server_step", "nsat_server_poll", "nsat_server_stats", "nsat_gen_random_dag",
     "nsat_gen_lfsr_stop", "nsat_server_program_check", "nsat_greedy_solve", "nsat_greedy_image",
-    "nsat_autotune", "nsat_autotune_reset", "nsat_probe_gather_peak",
+    "nsat_autotune", "nsat_autotune_reset", "nsat_probe_gather_peak", "nsat_server_tune",
 ]
 
 _lib = None
@@ -200,14 +213,15 @@ def lib():
         L.nsat_greedy_solve.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(GreedyOpts), C.POINTER(GreedyResult)]
         L.nsat_greedy_image.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_char_p, U64P, C.c_uint64]
         L.nsat_server_create.argtypes = [C.c_void_p, C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]
+        L.nsat_server_tune.argtypes = [C.c_void_p, C.POINTER(ServeTuneOpts), C.POINTER(ServeTuneResult)]
         L.nsat_server_destroy.argtypes = [C.c_void_p]
         L.nsat_server_destroy.restype = None
         L.nsat_server_submit.argtypes = [C.c_void_p, C.POINTER(JobDesc), C.POINTER(C.c_uint64)]
         L.nsat_server_step.argtypes = [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.nsat_server_poll.argtypes = [C.c_void_p, C.POINTER(JobResult), C.c_uint32, C.POINTER(C.c_uint32)]
         L.nsat_server_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
-        L.nsat_server_program_check.argtypes = [C.POINTER(CircuitDesc), C.c_uint32, C.c_uint64, U32P, U32P,
-                                                U32P]
+        L.nsat_server_program_check.argtypes = [C.POINTER(CircuitDesc), C.c_uint32, C.c_uint32, C.c_uint64, U32P,
+                                                U32P, U32P]
         L.nsat_gen_random_dag.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, U32P,
                                           C.c_uint32, U32P, C.c_uint32, U32P, U32P]
         L.nsat_gen_lfsr_stop.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, U32P, C.c_uint32, U32P,
@@ -410,6 +424,18 @@ class CircuitHandle:
 
 
 KINDS = {"sat": 0, "qsat": 1, "stop": 2}
+SERVE_SHAPES = 6     # NSAT_SERVE_SHAPES
+
+
+def server_tune(ctx, jobs=0, persist=False, retune=False, seed=0):
+    """nsat_server_tune: times every interpreter shape and four epoch
+    budgets on a seeded calibration set; returns the choice and the rates."""
+    o = ServeTuneOpts(jobs, 1 if persist else 0, 1 if retune else 0, 0, seed)
+    r = ServeTuneResult()
+    ctx._check(lib().nsat_server_tune(ctx.h, C.byref(o), C.byref(r)), "server_tune")
+    return {"shape": r.shape, "from_cache": bool(r.from_cache), "epoch_budget": r.epoch_budget,
+            "lut_words_per_s": list(r.lut_words_per_s), "budget_solves_per_s": list(r.budget_solves_per_s),
+            "budget_epoch_ms": list(r.budget_epoch_ms), "tune_ms": r.tune_ms}
 
 
 class Server:
@@ -417,10 +443,12 @@ class Server:
 
     def __init__(self, ctx, arena_bytes=0, max_active=0, max_queue=0, max_slice_tiles=0,
                  first_slice_tiles=0, epoch_budget=0, build_threads=0, tier_threads=0, tier_min_ms=0,
-                 tier_wait=False):
+                 tier_wait=False, shape=0):
+        """shape: interpreter shape 1..SERVE_SHAPES (include/nsat.h), 0 = the
+        one tuned for this GPU (nsat_server_tune) or the default."""
         self.ctx = ctx
         o = ServerOpts(arena_bytes, max_active, max_queue, max_slice_tiles, first_slice_tiles, epoch_budget,
-                       build_threads, tier_threads, tier_min_ms, 1 if tier_wait else 0)
+                       build_threads, tier_threads, tier_min_ms, 1 if tier_wait else 0, shape, 0)
         h = C.c_void_p()
         ctx._check(lib().nsat_server_create(ctx.h, C.byref(o), C.byref(h)), "server_create")
         self.h = h
@@ -574,13 +602,14 @@ def format_circuit(n, gates, outputs, quants=None):
 KIND = {"sat": 0, "qsat": 1, "table": 2}
 
 
-def server_program_check(circ, kind="sat", seed=1):
+def server_program_check(circ, kind="sat", seed=1, shape=0):
     """Host-only check of a job's interpreter program (include/nsat.h
-    nsat_server_program_check); returns (slots, luts, nops), raises on a
-    mismatch."""
+    nsat_server_program_check) for a server of `shape` (0 = the default);
+    returns (slots, luts, nops), raises on a mismatch."""
     d = desc_of(circ.n, circ.gates, circ.outputs)
     sl, lu, no = C.c_uint32(), C.c_uint32(), C.c_uint32()
-    rc = lib().nsat_server_program_check(C.byref(d), KINDS[kind], seed, C.byref(sl), C.byref(lu), C.byref(no))
+    rc = lib().nsat_server_program_check(C.byref(d), KINDS[kind], shape, seed, C.byref(sl), C.byref(lu),
+                                         C.byref(no))
     if rc != 0:
         raise NsatError("server_program_check: %s" % lib().nsat_strerror(rc).decode(), rc)
     return sl.value, lu.value, no.value

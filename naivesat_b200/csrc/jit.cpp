@@ -244,6 +244,12 @@ int jit_get(int device, const std::string& src, const std::vector<std::string>& 
 
 std::string jit_cache_dir() { return cache_dir(); }
 
+std::string jit_cache_dir_created() {
+    const std::string d = cache_dir();
+    mkdirs(d);
+    return d;
+}
+
 uint64_t jit_fnv(const std::string& s) { return fnv(s); }
 
 }  // namespace nsat

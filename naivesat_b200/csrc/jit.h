@@ -52,6 +52,8 @@ int jit_compile_only(const std::string& src, std::string* log, double* ms, std::
 // Directory of the on-disk kernel cache (NSAT_JIT_CACHE, else the user's
 // cache directory).
 std::string jit_cache_dir();
+// The same directory, created if it does not exist yet.
+std::string jit_cache_dir_created();
 
 // FNV-1a 64 of a byte string (cache keys).
 uint64_t jit_fnv(const std::string& s);

@@ -32,6 +32,7 @@
 
 #include "circuit.h"
 #include "internal.h"
+#include "jit.h"
 #include "lutmap.h"
 #include "nsat.h"
 #include "qreducer.h"
@@ -44,6 +45,7 @@ using namespace nsat;
 namespace {
 
 constexpr uint32_t kMaxActive = 512;
+constexpr uint32_t kDefaultShape = 0;        // index into kSrvShapes when nothing was tuned
 constexpr size_t kValsCap = 256 * 1024;      // QSAT tile values per epoch
 constexpr double kInterpRate = 1.5e12;        // interpreter LUT-words/s (measured), for the tiering estimate
 
@@ -91,7 +93,7 @@ struct Arena {
 };
 
 // LUT cover of the requested outputs as an interpreter program:
-// - scheduled into groups of SRV_GROUP instructions none of which reads
+// - scheduled into groups of `group` instructions none of which reads
 //   another's result (the kernel loads a whole group's operands before it
 //   stores any result): each group takes the lowest-numbered ready LUTs, so
 //   the original topological order, and with it the live set, is kept; a NOP
@@ -107,7 +109,8 @@ struct Program {
     uint32_t nops = 0;
 };
 
-bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool raw, Program* p, std::string* err) {
+bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool raw, uint32_t group, Program* p,
+                   std::string* err) {
     LutNet net = map_luts(c, which, raw, kCutLeavesServed);
     const uint32_t W = c.wires();
     const size_t L = net.luts.size();
@@ -130,20 +133,20 @@ bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool ra
     // groups of LUT indices (-1: NOP)
     std::set<uint32_t> ready;
     for (size_t k = 0; k < L; k++) if (!pending[k]) ready.insert((uint32_t)k);
-    std::vector<std::array<int64_t, SRV_GROUP>> groups;
+    std::vector<std::array<int64_t, SRV_MAX_GROUP>> groups;
     size_t done = 0;
     while (done < L) {
-        std::array<int64_t, SRV_GROUP> grp;
+        std::array<int64_t, SRV_MAX_GROUP> grp;
         grp.fill(-1);
         int used = 0;
-        while (used < SRV_GROUP && !ready.empty()) {
+        while (used < (int)group && !ready.empty()) {
             grp[used++] = *ready.begin();
             ready.erase(ready.begin());
         }
         for (int k = 0; k < used; k++) {
             for (uint32_t u : users[grp[k]]) if (--pending[u] == 0) ready.insert(u);
         }
-        p->nops += SRV_GROUP - used;
+        p->nops += group - used;
         done += used;
         groups.push_back(grp);
     }
@@ -160,7 +163,7 @@ bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool ra
     for (uint32_t i = c.n; i-- > 0;) if (last[i] < 0) freel.push_back(i);   // unread inputs
     const uint32_t scratch = next++;       // NOP operands and target
     p->ins.clear();
-    p->ins.reserve(groups.size() * SRV_GROUP);
+    p->ins.reserve(groups.size() * group);
     for (size_t g = 0; g < groups.size(); g++) {
         // operands read for the last time in this group free their slots first
         for (int64_t q : groups[g]) {
@@ -174,7 +177,8 @@ bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool ra
                 }
             }
         }
-        for (int64_t q : groups[g]) {
+        for (uint32_t k = 0; k < group; k++) {
+            const int64_t q = groups[g][k];
             uint32_t a = scratch, b = scratch, cc = scratch, d = scratch, tt = 0;
             if (q >= 0) {
                 const Lut& X = net.luts[q];
@@ -291,6 +295,7 @@ struct nsat_server {
     NsatJoinState* h_join = nullptr;
     uint64_t epochs = 0, launches = 0;
     uint64_t launched = 0;   // epochs launched (the sequence number of the last one)
+    uint32_t shape = 0;      // interpreter shape (index into kSrvShapes)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic the server issued
     double device_ms = 0;
     // builder threads: programs are built off the caller's thread
@@ -373,7 +378,7 @@ int capture_graph(nsat_server* s, EpochBuf& b, uint32_t narrow, uint32_t wide, c
     int per_sm[2] = {0, 0};
     const uint32_t slots[2] = {narrow, wide};
     for (int c = 0; c < (wide ? 2 : 1); c++)
-        if (nsat_serve_occupancy(slots[c], &per_sm[c]) || per_sm[c] < 1)
+        if (nsat_serve_occupancy(slots[c], s->shape, &per_sm[c]) || per_sm[c] < 1)
             return ctx_fail(s->ctx, NSAT_EUNSUPPORTED, "interpreter does not fit with " + std::to_string(slots[c]) + " slots");
     b.grid = per_sm[0] * ctx_sm_count(s->ctx);
     cudaGraph_t g = nullptr;
@@ -385,10 +390,11 @@ int capture_graph(nsat_server* s, EpochBuf& b, uint32_t narrow, uint32_t wide, c
     if (wide) {
         cudaEventRecord(s->fork, st);
         cudaStreamWaitEvent(s->cap2, s->fork, 0);
-        rc |= nsat_launch_serve_epoch(b.d_hdr, b.d_jobs, wide, b.d_vals, per_sm[1] * ctx_sm_count(s->ctx), 1, s->cap2);
+        rc |= nsat_launch_serve_epoch(b.d_hdr, b.d_jobs, wide, b.d_vals, per_sm[1] * ctx_sm_count(s->ctx), 1, s->shape,
+                                      s->cap2);
         cudaEventRecord(s->join, s->cap2);
     }
-    rc |= nsat_launch_serve_epoch(b.d_hdr, b.d_jobs, narrow, b.d_vals, b.grid, 0, st);
+    rc |= nsat_launch_serve_epoch(b.d_hdr, b.d_jobs, narrow, b.d_vals, b.grid, 0, s->shape, st);
     if (wide) cudaStreamWaitEvent(st, s->join, 0);
     cudaMemcpyAsync(b.h_jobs, b.d_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(b.h_vals, b.d_vals, kValsCap, cudaMemcpyDeviceToHost, st);
@@ -439,7 +445,7 @@ int admit(nsat_server* s, Job* j) {
     r.prog = (const SrvIns*)(s->arena.base + j->prog_off);
     r.outs = (const uint16_t*)(s->arena.base + j->outs_off);
     r.table = tbytes ? (srv_u64*)(s->arena.base + j->table_off) : nullptr;
-    r.ngroups = (uint32_t)(j->prog.ins.size() / SRV_GROUP);
+    r.ngroups = (uint32_t)(j->prog.ins.size() / kSrvShapes[s->shape].group);
     r.nslots = j->prog.nslots;
     r.kind = j->kind;
     r.nb = j->nb;
@@ -528,7 +534,7 @@ void builder_loop(nsat_server* s, bool raw) {
         }
         std::string err;
         int st = 1;
-        if (!build_program(j->circ, j->which, raw, &j->prog, &err)) {
+        if (!build_program(j->circ, j->which, raw, kSrvShapes[s->shape].group, &j->prog, &err)) {
             st = NSAT_EUNSUPPORTED;
         } else {
             // a job that could never be admitted is answered with an error
@@ -650,6 +656,33 @@ void tier_loop(nsat_server* s, nsat_opts copts) {
 
 }  // namespace
 
+namespace {
+
+std::string tuned_path(nsat_ctx* ctx) {
+    std::string k = "serve_tune1|";
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx_device(ctx)) == cudaSuccess)
+        k += std::string(prop.name) + "|" + std::to_string(prop.multiProcessorCount);
+    char hex[32];
+    snprintf(hex, sizeof(hex), "%016llx", (unsigned long long)jit_fnv(k));
+    return jit_cache_dir() + "/serve_tune_" + hex + ".txt";
+}
+
+bool read_tuned(nsat_ctx* ctx, uint32_t* shape, uint64_t* budget) {
+    FILE* f = fopen(tuned_path(ctx).c_str(), "r");
+    if (!f) return false;
+    unsigned sh = 0;
+    unsigned long long b = 0;
+    const int got = fscanf(f, "%u %llu", &sh, &b);
+    fclose(f);
+    if (got != 2 || sh < 1 || sh > SRV_NSHAPES || b == 0) return false;
+    *shape = sh;
+    *budget = b;
+    return true;
+}
+
+}  // namespace
+
 extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, nsat_server** out) {
     if (!ctx || !out) return NSAT_EINVAL;
     *out = nullptr;
@@ -662,7 +695,18 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     if (!s->opts.max_queue) s->opts.max_queue = 1u << 20;
     if (!s->opts.max_slice_tiles) s->opts.max_slice_tiles = 4096;
     if (!s->opts.first_slice_tiles) s->opts.first_slice_tiles = 1;
+    if (s->opts.shape > SRV_NSHAPES) return ctx_fail(ctx, NSAT_EINVAL, "no such interpreter shape");
+    if (!s->opts.shape || !s->opts.epoch_budget) {
+        // the tuned choice for this GPU, if one was persisted
+        uint32_t shape = 0;
+        uint64_t budget = 0;
+        if (read_tuned(ctx, &shape, &budget)) {
+            if (!s->opts.shape) s->opts.shape = shape;
+            if (!s->opts.epoch_budget) s->opts.epoch_budget = budget;
+        }
+    }
     if (!s->opts.epoch_budget) s->opts.epoch_budget = 48000000;
+    s->shape = s->opts.shape ? s->opts.shape - 1 : kDefaultShape;
     SCK(cudaSetDevice(ctx_device(ctx)));
     SCK(cudaMalloc(&s->arena.base, s->opts.arena_bytes));
     s->arena.cap = s->opts.arena_bytes;
@@ -830,7 +874,7 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
     b.h_hdr->njobs = k;
     b.h_hdr->n_narrow = (uint32_t)sel[0].size();
     b.h_hdr->hi_mul = 65536;
-    b.h_hdr->slot_bytes = SRV_SLOT_BYTES;
+    b.h_hdr->slot_bytes = srv_slot_bytes(s->shape);
     if (sel[0].empty()) narrow = 16;    // only wide jobs: the narrow launch finds nothing
     cudaGraphExec_t& ge = b.graphs[{narrow, wide}];
     if (!ge) {
@@ -1078,12 +1122,14 @@ extern "C" int nsat_server_stats(nsat_server* s, nsat_server_stats_t* st) {
     st->launches = s->launches;
     st->h2d_bytes = s->h2d_bytes;
     st->d2h_bytes = s->d2h_bytes;
+    st->shape = s->shape + 1;
     return NSAT_OK;
 }
 
-extern "C" int nsat_server_program_check(const nsat_circuit_desc* cd, uint32_t kind, uint64_t seed, uint32_t* slots,
-                                         uint32_t* luts, uint32_t* nops) {
-    if (!cd || kind > 2) return NSAT_EINVAL;
+extern "C" int nsat_server_program_check(const nsat_circuit_desc* cd, uint32_t kind, uint32_t shape, uint64_t seed,
+                                         uint32_t* slots, uint32_t* luts, uint32_t* nops) {
+    if (!cd || kind > 2 || shape > SRV_NSHAPES) return NSAT_EINVAL;
+    const uint32_t G = kSrvShapes[shape ? shape - 1 : kDefaultShape].group;
     Circuit c = circuit_from_desc(cd);
     if (!c.validate().empty()) return NSAT_EINVAL;
     std::vector<uint32_t> which;
@@ -1091,7 +1137,7 @@ extern "C" int nsat_server_program_check(const nsat_circuit_desc* cd, uint32_t k
     else which.push_back(0);
     Program p;
     std::string err;
-    if (!build_program(c, which, false, &p, &err)) return NSAT_EUNSUPPORTED;
+    if (!build_program(c, which, false, G, &p, &err)) return NSAT_EUNSUPPORTED;
     if (slots) *slots = p.nslots;
     if (luts) *luts = p.luts;
     if (nops) *nops = p.nops;
@@ -1114,9 +1160,9 @@ extern "C" int nsat_server_program_check(const nsat_circuit_desc* cd, uint32_t k
             const uint64_t a = wv[g.i0], b = wv[g.i1];
             wv[c.n + k] = g.func == AND ? (a & b) : g.func == NOR ? ~(a | b) : g.func == NIMPL ? (a & ~b) : (a ^ b);
         }
-        for (size_t g0 = 0; g0 < p.ins.size(); g0 += SRV_GROUP) {
-            uint64_t d[SRV_GROUP];
-            for (int k = 0; k < SRV_GROUP; k++) {
+        for (size_t g0 = 0; g0 < p.ins.size(); g0 += G) {
+            uint64_t d[SRV_MAX_GROUP];
+            for (uint32_t k = 0; k < G; k++) {
                 const SrvIns& r = p.ins[g0 + k];
                 const uint64_t a = sv[r.ab & 0xffff], b = sv[r.ab >> 16], cc = sv[r.cd & 0xffff];
                 uint64_t y = 0;
@@ -1127,7 +1173,7 @@ extern "C" int nsat_server_program_check(const nsat_circuit_desc* cd, uint32_t k
                 }
                 d[k] = y;
             }
-            for (int k = 0; k < SRV_GROUP; k++) sv[p.ins[g0 + k].cd >> 16] = d[k];
+            for (uint32_t k = 0; k < G; k++) sv[p.ins[g0 + k].cd >> 16] = d[k];
         }
         for (size_t j = 0; j < which.size(); j++) {
             const Output& o = c.outputs[which[j]];
@@ -1137,5 +1183,157 @@ extern "C" int nsat_server_program_check(const nsat_circuit_desc* cd, uint32_t k
             if (got != exp) return NSAT_EINVAL;
         }
     }
+    return NSAT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner of the interpreter shape and the epoch budget
+
+namespace {
+
+struct CalJob {
+    std::vector<uint32_t> gates, outs;
+    uint32_t n = 0;
+    uint64_t luts = 0;
+};
+
+// Serves every calibration job (SAT, count mode) on a new server with the
+// given shape and budget; returns LUT-words evaluated, device ms, wall ms
+// and epochs, or a status.
+int serve_calibration(nsat_ctx* ctx, const std::vector<CalJob>& jobs, uint32_t shape, uint64_t budget,
+                      double* lut_words, double* dev_ms, double* wall_ms, uint64_t* epochs) {
+    nsat_server_opts o{};
+    o.shape = shape;
+    o.epoch_budget = budget;
+    o.tier_min_ms = 0xffffffffu;      // the interpreter alone
+    nsat_server* s = nullptr;
+    if (int rc = nsat_server_create(ctx, &o, &s)) return rc;
+    const double t0 = now_ms();
+    for (size_t i = 0; i < jobs.size(); i++) {
+        nsat_job_desc d{};
+        d.kind = SRV_SAT;
+        d.circuit = nsat_circuit_desc{jobs[i].n, (uint32_t)(jobs[i].gates.size() / 3), jobs[i].gates.data(), 1,
+                                      jobs[i].outs.data()};
+        d.tag = i;
+        d.flags = NSAT_JOB_FIND_ALL;
+        uint64_t id = 0;
+        if (int rc = nsat_server_submit(s, &d, &id)) {
+            nsat_server_destroy(s);
+            return rc;
+        }
+    }
+    std::vector<nsat_job_result> res(jobs.size());
+    size_t got = 0;
+    *lut_words = 0;
+    for (;;) {
+        uint32_t active = 0, queued = 0, k = 0;
+        if (int rc = nsat_server_step(s, &active, &queued)) {
+            nsat_server_destroy(s);
+            return rc;
+        }
+        nsat_server_poll(s, res.data(), (uint32_t)res.size(), &k);
+        for (uint32_t i = 0; i < k; i++) {
+            if (res[i].status != NSAT_OK) {
+                nsat_server_destroy(s);
+                return res[i].status;
+            }
+            *lut_words += (double)res[i].tiles * 1024.0 * (double)jobs[res[i].tag].luts;
+        }
+        got += k;
+        if (got == jobs.size() && active == 0 && queued == 0) break;
+    }
+    *wall_ms = now_ms() - t0;
+    nsat_server_stats_t st{};
+    nsat_server_stats(s, &st);
+    *dev_ms = st.device_ms;
+    *epochs = st.epochs;
+    nsat_server_destroy(s);
+    return NSAT_OK;
+}
+
+}  // namespace
+
+extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts, nsat_serve_tune_result* res) {
+    if (!ctx || !res) return NSAT_EINVAL;
+    memset(res, 0, sizeof(*res));
+    const double t0 = now_ms();
+    nsat_serve_tune_opts o{};
+    if (opts) o = *opts;
+    if (o.persist && !o.retune) {
+        uint32_t shape = 0;
+        uint64_t budget = 0;
+        if (read_tuned(ctx, &shape, &budget)) {
+            res->shape = shape;
+            res->epoch_budget = budget;
+            res->from_cache = 1;
+            res->tune_ms = now_ms() - t0;
+            return NSAT_OK;
+        }
+    }
+    // the calibration set: random DAGs of the serving generator, 18-28
+    // inputs (the larger ones carry the work) and 100-4000 gates, log-uniform
+    const uint32_t njobs = o.jobs ? o.jobs : 24;
+    uint64_t st = o.seed ? o.seed : 0x5E7E5E7Eull;
+    auto rnd = [&st]() {
+        st += 0x9E3779B97F4A7C15ull;
+        uint64_t z = st;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    std::vector<CalJob> jobs(njobs);
+    for (uint32_t i = 0; i < njobs; i++) {
+        CalJob& j = jobs[i];
+        j.n = 18 + (uint32_t)(rnd() % 11);
+        const double u = (double)(rnd() >> 11) / (double)(1ull << 53);
+        const uint32_t g = (uint32_t)std::exp(std::log(100.0) + u * (std::log(4000.0) - std::log(100.0)));
+        j.gates.assign(3 * g, 0);
+        j.outs.assign(2, 0);
+        uint32_t gn = 0, on = 0;
+        if (nsat_gen_random_dag(rnd(), j.n, g, 64, 1, j.gates.data(), g, j.outs.data(), 1, &gn, &on) != NSAT_OK)
+            return NSAT_EINVAL;
+        j.gates.resize(3 * gn);
+        const nsat_circuit_desc d{j.n, gn, j.gates.data(), 1, j.outs.data()};
+        const Circuit c = circuit_from_desc(&d);
+        j.luts = map_luts(c, {0}, ctx_no_optimize(ctx), kCutLeavesServed).luts.size();
+    }
+    // every shape at the default budget, by device time
+    double best = -1;
+    for (uint32_t sh = 1; sh <= SRV_NSHAPES; sh++) {
+        double lw = 0, dms = 0, wms = 0;
+        uint64_t ep = 0;
+        if (int rc = serve_calibration(ctx, jobs, sh, 48000000, &lw, &dms, &wms, &ep)) return rc;
+        res->lut_words_per_s[sh - 1] = dms > 0 ? lw / (dms * 1e-3) : 0;
+        if (res->lut_words_per_s[sh - 1] > best) {
+            best = res->lut_words_per_s[sh - 1];
+            res->shape = sh;
+        }
+    }
+    // the epoch budget for that shape, by wall clock, under the epoch-length cap
+    static const uint64_t budgets[4] = {12000000, 24000000, 48000000, 96000000};
+    double best_rate = -1;
+    res->epoch_budget = 48000000;
+    for (int b = 0; b < 4; b++) {
+        double lw = 0, dms = 0, wms = 0;
+        uint64_t ep = 0;
+        if (int rc = serve_calibration(ctx, jobs, res->shape, budgets[b], &lw, &dms, &wms, &ep)) return rc;
+        res->budget_solves_per_s[b] = wms > 0 ? njobs / (wms * 1e-3) : 0;
+        res->budget_epoch_ms[b] = ep ? wms / (double)ep : 0;
+        if (res->budget_epoch_ms[b] <= 20.0 && res->budget_solves_per_s[b] > best_rate) {
+            best_rate = res->budget_solves_per_s[b];
+            res->epoch_budget = budgets[b];
+        }
+    }
+    if (o.persist) {
+        jit_cache_dir_created();
+        const std::string path = tuned_path(ctx), tmp = path + ".tmp";
+        FILE* f = fopen(tmp.c_str(), "w");
+        if (f) {
+            fprintf(f, "%u %llu\n", res->shape, (unsigned long long)res->epoch_budget);
+            fclose(f);
+            rename(tmp.c_str(), path.c_str());
+        }
+    }
+    res->tune_ms = now_ms() - t0;
     return NSAT_OK;
 }

@@ -4,21 +4,31 @@
 #include <stdint.h>
 #include <vector_types.h>
 
-// Geometry of the interpreter: each lane evaluates SRV_WORDS 32-bit words
-// per program pass (SRV_WORDS * 1024 assignments per warp), and a tile of
-// 2^SRV_TILE_BITS assignments takes 32 / SRV_WORDS passes.  A slot of a warp
-// is SRV_SLOT_BYTES of shared memory laid out [lane][word].
-#ifndef SRV_WORDS
-#define SRV_WORDS 4
-#endif
-#ifndef SRV_GROUP
-#define SRV_GROUP 4               // instructions issued together (mutually independent)
-#endif
-#define SRV_LOG_WORDS (SRV_WORDS == 4 ? 2 : 1)
-#define SRV_SLOT_BYTES (32 * SRV_WORDS * 4)
-#define SRV_MAX_SLOTS 384          // slots per warp (384 x 512 B = 192 KB of shared memory)
+// Geometry of the interpreter.  A shape fixes the words each lane evaluates
+// per program pass (W: W * 1024 assignments per warp), the size of the groups
+// of mutually independent instructions the program is scheduled into (G: a
+// group's operands are all loaded before any of its results is stored), and
+// how a LUT with a run-time truth table is evaluated: a 7-lop3 mux tree over
+// masks expanded from the table, or a jump on the warp-uniform table to one
+// lop3 with that table as its immediate.  A tile of 2^SRV_TILE_BITS
+// assignments takes 32 / W passes; a slot of a warp is 32 * W * 4 bytes of
+// shared memory laid out [lane][word].  The server picks one shape (option,
+// tuned and persisted per GPU, or the default) and builds its programs with
+// that shape's group size.
+struct SrvShape {
+    uint32_t words;      // W: 2 or 4
+    uint32_t group;      // G: 1, 2 or 4
+    uint32_t dispatch;   // 0: mux tree, 1: jump on the truth table
+};
+#define SRV_NSHAPES 6
+static const SrvShape kSrvShapes[SRV_NSHAPES] = {
+    {4, 4, 0}, {4, 1, 1}, {4, 2, 1}, {4, 4, 1}, {2, 1, 1}, {2, 2, 1},
+};
+#define SRV_MAX_GROUP 4
+#define SRV_MAX_SLOTS 384          // slots per warp (384 x 512 B = 192 KB of shared memory at W = 4)
 #define SRV_TILE_BITS 15           // assignments per warp tile
 #define SRV_MAX_NB 48              // enumeration bits a serving job may have
+inline uint32_t srv_slot_bytes(uint32_t shape) { return 32u * kSrvShapes[shape].words * 4u; }
 
 // One instruction: slot[d] = LUT(slot[a], slot[b], slot[c]), 16 bytes:
 //   ab = a | b << 16, cd = c | d << 16   (slot indices)
@@ -26,8 +36,8 @@
 //   a=x, b=y, c=z) spread so that bit k of tt is the sign bit of byte k of
 //   the 8-byte pair {thi, tlo}; the kernel expands mask k (all ones or all
 //   zeros) with one byte permute that replicates that sign bit.
-// Programs are sequences of groups of SRV_GROUP instructions none of which
-// reads another's result.
+// Programs are sequences of groups of G instructions (the shape's group
+// size) none of which reads another's result.
 struct SrvIns {
     uint32_t ab, cd, tlo, thi;
 };
@@ -41,8 +51,8 @@ enum { SRV_SAT = 0, SRV_QSAT = 1, SRV_TABLE = 2 };
 struct SrvEpoch {
     uint32_t njobs;
     uint32_t n_narrow;
-    uint32_t hi_mul;        // 65536 and SRV_SLOT_BYTES, read at run time so the
-    uint32_t slot_bytes;    // kernel's slot decode stays multiply-adds
+    uint32_t hi_mul;        // 65536 and the shape's slot bytes, read at run time so
+    uint32_t slot_bytes;    // the kernel's slot decode stays multiply-adds
     uint32_t pad[60];
 };
 #define SRV_NARROW_SLOTS 48
@@ -53,7 +63,7 @@ typedef unsigned long long srv_u64;   // the device atomics' 64-bit type
 
 struct SrvJob {
     // static
-    const SrvIns* prog;          // ngroups * SRV_GROUP instructions
+    const SrvIns* prog;          // ngroups * G instructions (G: the server shape's group size)
     const void* unused0;
     const uint16_t* outs;        // output slots (bit 15 = negated), nout of them
     srv_u64* table;             // TABLE: 2^np u64 entries (next|STOP<<n | 1<<32)

@@ -1,26 +1,29 @@
 // serve_kernels.cu -- the batched serving engine's kernel: a LOP3 bytecode
 // interpreter that evaluates many different circuits in one launch.
 //
-// Per-request NVRTC compilation costs 0.1-1.5 s per circuit, far more than
+// Per-request NVRTC compilation costs 0.06-0.7 s per circuit, far more than
 // the device work of most serving requests, so serving does not specialise
 // kernels: every job is a program of 3-input LUT instructions over "slots"
 // (the LUT cover of its circuit, scheduled into groups of independent
 // instructions and slot-allocated by liveness).  A CTA is one warp; each lane
-// evaluates SRV_WORDS words per program pass, and slot values live in the
-// warp's shared memory laid out [slot][lane][word] (128-bit accesses,
-// conflict-free).  A LUT with a run-time truth table is a 7-lop3 mux tree
-// over eight masks expanded from the truth table in the instruction record.
+// evaluates W words per program pass, and slot values live in the warp's
+// shared memory laid out [slot][lane][word] (conflict-free vector accesses).
 //
-// Cost per instruction and warp: 3 x 128-bit shared loads, one 128-bit
-// shared store, one uniform 128-bit load of the 16-byte record, 8 byte
-// permutes that expand the truth table into masks, 7 * SRV_WORDS lop3, and a
-// slot decode done with multiply-adds so that it runs on the FMA pipe, not on
-// the ALU pipe that bounds the kernel.
-// The L1 data pipe moves 512 bytes per 128-bit warp access, so the record is
-// kept at 16 bytes (a record of eight mask words cost 12 of the
-// instruction's 28 L1 cycles).  Groups of SRV_GROUP independent
-// instructions keep 3 * SRV_GROUP shared loads in flight, and the records of
-// the next group are loaded while the current one computes.
+// The kernel is instantiated for each shape of serve_common.h (W words per
+// lane, groups of G instructions, LUT evaluation by mux tree or by jump):
+// - mux tree: a LUT with a run-time truth table is 7 lop3 over eight masks
+//   that 8 byte permutes expand from the 16-byte record (W = 4: 28 lop3 and
+//   8 prmt per instruction and warp);
+// - jump: every lane of a warp runs the same program, so the truth table is
+//   warp-uniform; a switch over its 256 values jumps to one lop3 per word
+//   with the table as its immediate (W lop3 per instruction).
+// Either way an instruction reads three slots and writes one: 16 bytes of
+// shared-memory traffic per LUT-word, which bounds the interpreter at
+// 128 B/clk/SM / 16 B = 8 LUT-words per SM clock.
+// The slot decode is done with multiply-adds so that it runs on the FMA pipe.
+// A group of G independent instructions keeps 3 * G shared loads in flight,
+// and the records of the next group are loaded while the current one
+// computes.
 //
 // Scheduling is on the device: every warp starts at its own job of the epoch
 // table and claims tiles of that job's slice with an atomic cursor, moving on
@@ -37,12 +40,6 @@ typedef unsigned long long u64;
 
 namespace {
 
-constexpr int W = SRV_WORDS;
-constexpr int G = SRV_GROUP;
-constexpr int LOGW = SRV_LOG_WORDS;
-constexpr u32 ITERS = 32u / W;                 // program passes per tile
-static_assert(W == 2 || W == 4, "SRV_WORDS must be 2 or 4");
-static_assert((1 << LOGW) == W, "SRV_LOG_WORDS");
 
 template <int LUT>
 __device__ __forceinline__ u32 lop3(u32 a, u32 b, u32 c) {
@@ -92,12 +89,14 @@ __device__ __forceinline__ void transpose32(u32* a) {
     }
 }
 
+template <int W>
 struct Vals {
     u32 v[W];
 };
 
-__device__ __forceinline__ Vals lds(const char* p) {
-    Vals r;
+template <int W>
+__device__ __forceinline__ Vals<W> lds(const char* p) {
+    Vals<W> r;
     if constexpr (W == 4) {
         const uint4 t = *reinterpret_cast<const uint4*>(p);
         r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
@@ -108,7 +107,8 @@ __device__ __forceinline__ Vals lds(const char* p) {
     return r;
 }
 
-__device__ __forceinline__ void sts(char* p, const Vals& x) {
+template <int W>
+__device__ __forceinline__ void sts(char* p, const Vals<W>& x) {
     if constexpr (W == 4) *reinterpret_cast<uint4*>(p) = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
     else *reinterpret_cast<uint2*>(p) = make_uint2(x.v[0], x.v[1]);
 }
@@ -141,7 +141,6 @@ __device__ __forceinline__ u32 lut_mux(u32 a, u32 b, u32 c, const Lut& t) {
     return mux(a, mux(b, x67, x45), mux(b, x23, x01));
 }
 
-#ifdef SRV_DISPATCH
 // The truth table of a record as an 8-bit number: bit k of tt is the sign
 // bit of byte k of {thi, tlo}.  (x >> 7) has those bits at 0, 8, 16, 24, and
 // the product with 0x01020408 gathers them into bits 24..27 (every other
@@ -156,20 +155,21 @@ __device__ __forceinline__ u32 tt_of(u32 tlo, u32 thi) {
 // One LUT on W words with its truth table as the lop3 immediate: the table
 // is the same for the whole warp (every lane runs the same program), so the
 // switch is a uniform jump and each word costs one lop3.
-template <int T>
-__device__ __forceinline__ void lut_imm(const Vals& a, const Vals& b, const Vals& c, Vals& d) {
+template <int T, int W>
+__device__ __forceinline__ void lut_imm(const Vals<W>& a, const Vals<W>& b, const Vals<W>& c, Vals<W>& d) {
 #pragma unroll
     for (int w = 0; w < W; w++) d.v[w] = lop3<T>(a.v[w], b.v[w], c.v[w]);
 }
 
 #define SRV_CASE(t) \
-    case (t): lut_imm<(t)>(a, b, c, d); break;
+    case (t): lut_imm<(t), W>(a, b, c, d); break;
 #define SRV_CASE4(t) SRV_CASE(t) SRV_CASE((t) + 1) SRV_CASE((t) + 2) SRV_CASE((t) + 3)
 #define SRV_CASE16(t) SRV_CASE4(t) SRV_CASE4((t) + 4) SRV_CASE4((t) + 8) SRV_CASE4((t) + 12)
 #define SRV_CASE64(t) SRV_CASE16(t) SRV_CASE16((t) + 16) SRV_CASE16((t) + 32) SRV_CASE16((t) + 48)
 
-__device__ __forceinline__ Vals lut_switch(u32 tt, const Vals& a, const Vals& b, const Vals& c) {
-    Vals d;
+template <int W>
+__device__ __forceinline__ Vals<W> lut_switch(u32 tt, const Vals<W>& a, const Vals<W>& b, const Vals<W>& c) {
+    Vals<W> d;
     switch (tt & 255u) {
         SRV_CASE64(0)
         SRV_CASE64(64)
@@ -178,7 +178,6 @@ __device__ __forceinline__ Vals lut_switch(u32 tt, const Vals& a, const Vals& b,
     }
     return d;
 }
-#endif
 
 // Slot fields decoded with multiply-adds (FMA pipe) instead of masks and
 // shifts (ALU pipe, the kernel's bound): hi = x * km >> 32 with km = 65536,
@@ -192,6 +191,7 @@ __device__ __forceinline__ void fields(u32 x, const Dec& dc, u32* lo, u32* hi) {
 
 // Runs a job's program once on this lane's W words.  Sl is the warp's slot
 // area plus lane * W * 4.
+template <int W, int G, bool DISPATCH>
 __device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32 ngroups, char* __restrict__ Sl,
                                             const Dec& dc) {
     if (ngroups == 0) return;
@@ -200,16 +200,16 @@ __device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32
 #pragma unroll
     for (int k = 0; k < G; k++) cur[k] = __ldg(P + k);
     for (u32 g = 0; g < ngroups; g++) {
-        Vals a[G], b[G], c[G];
+        Vals<W> a[G], b[G], c[G];
         u32 dof[G];
 #pragma unroll
         for (int k = 0; k < G; k++) {
             u32 al, ah, cl, ch;
             fields(cur[k].x, dc, &al, &ah);
             fields(cur[k].y, dc, &cl, &ch);
-            a[k] = lds(Sl + al * dc.sb);
-            b[k] = lds(Sl + ah * dc.sb);
-            c[k] = lds(Sl + cl * dc.sb);
+            a[k] = lds<W>(Sl + al * dc.sb);
+            b[k] = lds<W>(Sl + ah * dc.sb);
+            c[k] = lds<W>(Sl + cl * dc.sb);
             dof[k] = ch * dc.sb;
         }
         const uint4* nx = P + (size_t)(g + 1 < ngroups ? g + 1 : g) * G;
@@ -218,24 +218,25 @@ __device__ __forceinline__ void run_program(const SrvIns* __restrict__ prog, u32
         for (int k = 0; k < G; k++) nxt[k] = __ldg(nx + k);
 #pragma unroll
         for (int k = 0; k < G; k++) {
-#ifdef SRV_DISPATCH
-            const Vals d = lut_switch(tt_of(cur[k].z, cur[k].w), a[k], b[k], c[k]);
-#else
-            const Lut t = expand(cur[k]);
-            Vals d;
+            Vals<W> d;
+            if constexpr (DISPATCH) {
+                d = lut_switch<W>(tt_of(cur[k].z, cur[k].w), a[k], b[k], c[k]);
+            } else {
+                const Lut t = expand(cur[k]);
 #pragma unroll
-            for (int w = 0; w < W; w++) d.v[w] = lut_mux(a[k].v[w], b[k].v[w], c[k].v[w], t);
-#endif
-            sts(Sl + dof[k], d);
+                for (int w = 0; w < W; w++) d.v[w] = lut_mux(a[k].v[w], b[k].v[w], c[k].v[w], t);
+            }
+            sts<W>(Sl + dof[k], d);
         }
 #pragma unroll
         for (int k = 0; k < G; k++) cur[k] = nxt[k];
     }
 }
 
-__device__ __forceinline__ Vals read_out(const char* Sl, const uint16_t* outs, u32 j) {
+template <int W>
+__device__ __forceinline__ Vals<W> read_out(const char* Sl, const uint16_t* outs, u32 j) {
     const uint16_t o = __ldg(outs + j);
-    Vals v = lds(Sl + (u32)(o & 0x7fffu) * SRV_SLOT_BYTES);
+    Vals<W> v = lds<W>(Sl + (u32)(o & 0x7fffu) * (32u * W * 4u));
     if (o & 0x8000u) {
 #pragma unroll
         for (int w = 0; w < W; w++) v.v[w] = ~v.v[w];
@@ -248,12 +249,14 @@ __device__ __forceinline__ Vals read_out(const char* Sl, const uint16_t* outs, u
 // bits from SRV_TILE_BITS up are the tile index.  Input slots are rewritten
 // every pass because the program reuses slots of inputs it has finished
 // reading.
+template <int W>
 __device__ __forceinline__ void set_inputs(const SrvJob* J, u64 tile_base, u32 it, u32 lane, char* Sl) {
+    constexpr int LOGW = W == 4 ? 2 : 1;
     const u32 nb = J->nb < SRV_MAX_NB ? J->nb : SRV_MAX_NB;
     for (u32 p = 0; p < nb; p++) {
         const int s = J->in_slot[p];
         if (s < 0) continue;
-        Vals v;
+        Vals<W> v;
 #pragma unroll
         for (int w = 0; w < W; w++) {
             u32 x;
@@ -264,13 +267,15 @@ __device__ __forceinline__ void set_inputs(const SrvJob* J, u64 tile_base, u32 i
             else x = 0u - (u32)((tile_base >> p) & 1ull);
             v.v[w] = x;
         }
-        sts(Sl + (u32)s * SRV_SLOT_BYTES, v);
+        sts<W>(Sl + (u32)s * (32u * W * 4u), v);
     }
 }
 
 // Evaluates tile `tile` of job `J` with this warp.
+template <int W, int G, bool DISPATCH>
 __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ Sl, u32 lane, uint8_t* __restrict__ vals,
                                         const Dec& dc) {
+    constexpr u32 ITERS = 32u / W;                 // program passes per tile
     const u64 tile_base = tile << SRV_TILE_BITS;     // first assignment of the tile
     const u32 kind = J->kind;
     const SrvIns* prog = J->prog;
@@ -282,17 +287,17 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
     const u64 allbits = J->allbits;
     const u32 dec_all = J->q0all;
     for (u32 it = 0; it < ITERS; it++) {
-        set_inputs(J, tile_base, it, lane, Sl);
-        run_program(prog, ngroups, Sl, dc);
+        set_inputs<W>(J, tile_base, it, lane, Sl);
+        run_program<W, G, DISPATCH>(prog, ngroups, Sl, dc);
         if (kind == SRV_SAT) {
-            const Vals y = read_out(Sl, J->outs, 0);
+            const Vals<W> y = read_out<W>(Sl, J->outs, 0);
 #pragma unroll
             for (int w = 0; w < W; w++) {
                 cnt += __popc(y.v[w]);
                 if (first == 0xffffffffu && y.v[w]) first = ((it * W + w) << 5) | (u32)(__ffs(y.v[w]) - 1);
             }
         } else if (kind == SRV_QSAT) {
-            const Vals yy = read_out(Sl, J->outs, 0);
+            const Vals<W> yy = read_out<W>(Sl, J->outs, 0);
 #pragma unroll
             for (int w = 0; w < W; w++) {
                 u32 y = yy.v[w];
@@ -324,7 +329,7 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
                 u32 o[32];
 #pragma unroll
                 for (int k = 0; k < 32; k++) {
-                    if ((u32)k < nout) o[k] = read_out(Sl, J->outs, k).v[w];
+                    if ((u32)k < nout) o[k] = read_out<W>(Sl, J->outs, k).v[w];
                     else o[k] = 0u;
                 }
                 stop_any |= o[nout - 1];
@@ -365,6 +370,7 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
 
 // One warp per CTA; the dynamic shared memory is max_slots * SRV_SLOT_BYTES.
 // cls 0 serves the epoch's narrow jobs, cls 1 its wide ones.
+template <int W, int G, bool DISPATCH>
 __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict__ hdr, SrvJob* __restrict__ jobs,
                                                   uint8_t* __restrict__ vals, u32 cls) {
     extern __shared__ __align__(16) char smem[];
@@ -389,27 +395,40 @@ __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict_
             continue;
         }
         dry = 0;
-        do_tile(J, tile, Sl, lane, vals, dc);
+        do_tile<W, G, DISPATCH>(J, tile, Sl, lane, vals, dc);
     }
+}
+
+typedef void (*EpochKernel)(const SrvEpoch*, SrvJob*, uint8_t*, u32);
+
+// the instantiation of each shape of kSrvShapes, in order
+EpochKernel kernel_of(uint32_t shape) {
+    static const EpochKernel k[SRV_NSHAPES] = {
+        serve_epoch<4, 4, false>, serve_epoch<4, 1, true>, serve_epoch<4, 2, true>,
+        serve_epoch<4, 4, true>,  serve_epoch<2, 1, true>, serve_epoch<2, 2, true>,
+    };
+    return shape < SRV_NSHAPES ? k[shape] : nullptr;
 }
 
 }  // namespace
 
 extern "C" int nsat_launch_serve_epoch(const SrvEpoch* hdr, SrvJob* jobs, uint32_t max_slots, uint8_t* vals,
-                                       int grid, uint32_t cls, cudaStream_t stream) {
+                                       int grid, uint32_t cls, uint32_t shape, cudaStream_t stream) {
     // the dynamic shared memory limit was raised by nsat_serve_occupancy
-    const size_t smem = (size_t)max_slots * SRV_SLOT_BYTES;
-    serve_epoch<<<grid, 32, smem, stream>>>(hdr, jobs, vals, cls);
+    const EpochKernel fn = kernel_of(shape);
+    if (!fn) return -1;
+    const size_t smem = (size_t)max_slots * srv_slot_bytes(shape);
+    fn<<<grid, 32, smem, stream>>>(hdr, jobs, vals, cls);
     return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 
-extern "C" int nsat_serve_occupancy(uint32_t max_slots, int* ctas_per_sm) {
-    if (max_slots > SRV_MAX_SLOTS) return -1;
-    const size_t smem = (size_t)max_slots * SRV_SLOT_BYTES;
-    const void* fn = (const void*)serve_epoch;
+extern "C" int nsat_serve_occupancy(uint32_t max_slots, uint32_t shape, int* ctas_per_sm) {
+    const EpochKernel fn = kernel_of(shape);
+    if (!fn || max_slots > SRV_MAX_SLOTS) return -1;
+    const size_t smem = (size_t)max_slots * srv_slot_bytes(shape);
     // the limit covers every slot count, so launches captured earlier stay valid
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, SRV_MAX_SLOTS * SRV_SLOT_BYTES) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SRV_MAX_SLOTS * srv_slot_bytes(shape)) != cudaSuccess)
         return -4;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32, smem) == cudaSuccess ? 0 : -4;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, (const void*)fn, 32, smem) == cudaSuccess ? 0 : -4;
 }

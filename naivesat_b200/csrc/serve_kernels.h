@@ -6,10 +6,11 @@
 #include "serve_common.h"
 
 extern "C" {
-// grid one-warp CTAs, each with max_slots * SRV_SLOT_BYTES of shared memory,
-// serving the epoch's narrow (cls 0) or wide (cls 1) jobs
+// grid one-warp CTAs of the interpreter of shape `shape` (kSrvShapes), each
+// with max_slots * srv_slot_bytes(shape) of shared memory, serving the
+// epoch's narrow (cls 0) or wide (cls 1) jobs
 int nsat_launch_serve_epoch(const SrvEpoch* hdr, SrvJob* jobs, uint32_t max_slots, uint8_t* vals, int grid,
-                            uint32_t cls, cudaStream_t stream);
-// raises the kernel's shared-memory limit for max_slots and reports CTAs per SM
-int nsat_serve_occupancy(uint32_t max_slots, int* ctas_per_sm);
+                            uint32_t cls, uint32_t shape, cudaStream_t stream);
+// raises that kernel's shared-memory limit for max_slots and reports CTAs per SM
+int nsat_serve_occupancy(uint32_t max_slots, uint32_t shape, int* ctas_per_sm);
 }

@@ -139,6 +139,17 @@ def test_server_program_matches_circuit(seed, n, g):
     assert nops <= luts // 4 + 8
 
 
+@pytest.mark.parametrize("shape", range(1, api.SERVE_SHAPES + 1))
+def test_server_programs_of_every_shape(shape):
+    """Every interpreter shape's group size gives a program that computes the
+    circuit (groups of 1, 2 or 4 independent instructions)."""
+    for seed, n, g in [(1, 34, 4000), (4, 26, 600), (9, 18, 60)]:
+        c = W.random_dag(seed, n, g, output="live")
+        slots, luts, nops = api.server_program_check(c, "sat", seed=seed, shape=shape)
+        assert slots <= 384 and luts > 0
+    api.server_program_check(W.config("c3a"), "stop", shape=shape)
+
+
 def test_server_program_check_on_config_circuits():
     for name, kind in [("c0", "sat"), ("c1", "sat"), ("c2a", "qsat"), ("c2c", "qsat"), ("c3a", "stop"),
                        ("c3b", "stop")]:

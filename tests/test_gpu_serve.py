@@ -256,3 +256,34 @@ def test_continuous_batching_jobs_arrive_while_others_run(ctx):
     assert len(admitted_late) >= 2, [(res[t]["admit_ms"], res[t]["done_ms"]) for t in wait_tags]
     # and every waiter still ran while the long jobs were active
     assert any(overlaps(t, L) for t in wait_tags for L in range(len(longs)))
+
+
+@pytest.mark.parametrize("shape", range(1, api.SERVE_SHAPES + 1))
+def test_every_interpreter_shape_matches_oracle(ctx, shape):
+    """The same mixed batch under each interpreter shape (words per lane,
+    group size, mux tree or jump on the truth table): every answer equals
+    the oracle's."""
+    reqs = small_mix(24, 61)
+    srv = api.Server(ctx, shape=shape, tier_min_ms=0xFFFFFFFF)
+    assert srv.stats()["shape"] == shape
+    submit_all(srv, reqs)
+    res = {r["tag"]: r for r in srv.run_all()}
+    srv.close()
+    for i, r in enumerate(reqs):
+        exp = expected(r)
+        assert project(res[i], exp) == exp, (shape, i, r["kind"], res[i], exp)
+
+
+def test_server_tune_persists_and_is_used(ctx, tmp_path, monkeypatch):
+    """nsat_server_tune times every shape and four epoch budgets, persists
+    its choice for this GPU, and a server created with the defaults uses it."""
+    monkeypatch.setenv("NSAT_JIT_CACHE", str(tmp_path))
+    t = api.server_tune(ctx, jobs=8, persist=True)
+    assert 1 <= t["shape"] <= api.SERVE_SHAPES and not t["from_cache"]
+    assert all(x > 0 for x in t["lut_words_per_s"])
+    assert t["epoch_budget"] in (12000000, 24000000, 48000000, 96000000)
+    again = api.server_tune(ctx, persist=True)
+    assert again["from_cache"] and again["shape"] == t["shape"] and again["epoch_budget"] == t["epoch_budget"]
+    srv = api.Server(ctx)
+    assert srv.stats()["shape"] == t["shape"]
+    srv.close()
