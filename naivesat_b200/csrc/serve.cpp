@@ -223,7 +223,8 @@ struct Job {
     uint32_t n = 0, nb = 0, d = 0;   // inputs, enumeration bits, dummy bits
     uint32_t f = 0, m = 0;           // QSAT first block length, unit level
     uint64_t total_tiles = 0;
-    uint64_t cursor = 0;             // tiles whose results were processed
+    uint64_t cursor = 0;             // the device cursor as of the last processed epoch
+    uint32_t slot = UINT32_MAX;      // entry of the server's state array
     uint64_t sched = 0;              // tiles handed to launched epochs
     uint64_t slice = 1;
     uint32_t inflight = 0;           // launched epochs holding a slice whose results are not processed yet
@@ -265,6 +266,7 @@ struct EpochBuf {
     uint8_t* d_vals = nullptr;
     SrvEpoch* h_hdr = nullptr;
     SrvJob* h_jobs = nullptr;
+    SrvState* h_state = nullptr;     // the state array as the epoch left it
     uint8_t* h_vals = nullptr;
     // epoch graphs by (narrow slots, wide slots; 0 = no wide launch)
     std::map<std::pair<uint32_t, uint32_t>, cudaGraphExec_t> graphs;
@@ -291,6 +293,9 @@ struct nsat_server {
     int cur = 0;       // buffer the next epoch is built in
     cudaStream_t cap = nullptr, cap2 = nullptr;   // streams the epoch graphs are captured on (never run work)
     cudaEvent_t fork = nullptr, join = nullptr;
+    SrvState* d_state = nullptr;     // kMaxActive persistent job states (cursor, results)
+    SrvState* h_state_init = nullptr;
+    std::vector<uint32_t> free_slots;
     NsatJoinState* d_join = nullptr;
     NsatJoinState* h_join = nullptr;
     uint64_t epochs = 0, launches = 0;
@@ -347,6 +352,7 @@ struct nsat_server {
             cudaFree(b.d_vals);
             cudaFreeHost(b.h_hdr);
             cudaFreeHost(b.h_jobs);
+            cudaFreeHost(b.h_state);
             cudaFreeHost(b.h_vals);
             if (b.ev0) cudaEventDestroy(b.ev0);
             if (b.ev1) cudaEventDestroy(b.ev1);
@@ -356,6 +362,8 @@ struct nsat_server {
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         cudaFree(arena.base);
+        cudaFree(d_state);
+        cudaFreeHost(h_state_init);
         cudaFree(d_join);
         cudaFreeHost(h_join);
     }
@@ -396,7 +404,7 @@ int capture_graph(nsat_server* s, EpochBuf& b, uint32_t narrow, uint32_t wide, c
     }
     rc |= nsat_launch_serve_epoch(b.d_hdr, b.d_jobs, narrow, b.d_vals, b.grid, 0, s->shape, st);
     if (wide) cudaStreamWaitEvent(st, s->join, 0);
-    cudaMemcpyAsync(b.h_jobs, b.d_jobs, sizeof(SrvJob) * kMaxActive, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(b.h_state, s->d_state, sizeof(SrvState) * kMaxActive, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(b.h_vals, b.d_vals, kValsCap, cudaMemcpyDeviceToHost, st);
     cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (rc || ce != cudaSuccess) {
@@ -425,12 +433,15 @@ int admit(nsat_server* s, Job* j) {
     size_t offs[4] = {0, 0, 0, 0};
     const size_t sizes[4] = {pbytes, obytes, tbytes, tbytes};
     const int parts = tbytes ? 4 : 2;
+    if (s->free_slots.empty()) return 1;
     for (int i = 0; i < parts; i++) {
         if (!s->arena.alloc(sizes[i], &offs[i])) {
             for (int k = 0; k < i; k++) s->arena.release(offs[k], sizes[k]);
             return 1;
         }
     }
+    j->slot = s->free_slots.back();
+    s->free_slots.pop_back();
     j->prog_off = offs[0]; j->outs_off = offs[1];
     j->table_off = offs[2]; j->table2_off = offs[3];
     j->reserve = pbytes + obytes + 2 * tbytes;
@@ -439,11 +450,14 @@ int admit(nsat_server* s, Job* j) {
     SCK(cudaMemcpyAsync(s->arena.base + j->prog_off, j->prog.ins.data(), j->prog.ins.size() * sizeof(SrvIns),
                         cudaMemcpyHostToDevice, st));
     SCK(cudaMemcpyAsync(s->arena.base + j->outs_off, j->prog.outs.data(), j->prog.outs.size() * 2, cudaMemcpyHostToDevice, st));
-    s->h2d_bytes += j->prog.ins.size() * sizeof(SrvIns) + j->prog.outs.size() * 2;
+    SCK(cudaMemcpyAsync(s->d_state + j->slot, s->h_state_init, sizeof(SrvState), cudaMemcpyHostToDevice, st));
+    s->h2d_bytes += j->prog.ins.size() * sizeof(SrvIns) + j->prog.outs.size() * 2 + sizeof(SrvState);
     SrvJob& r = j->rec;
     memset(&r, 0, sizeof(r));
     r.prog = (const SrvIns*)(s->arena.base + j->prog_off);
     r.outs = (const uint16_t*)(s->arena.base + j->outs_off);
+    r.st = s->d_state + j->slot;
+    r.flags = j->find_all ? SRV_JOB_FIND_ALL : 0u;
     r.table = tbytes ? (srv_u64*)(s->arena.base + j->table_off) : nullptr;
     r.ngroups = (uint32_t)(j->prog.ins.size() / kSrvShapes[s->shape].group);
     r.nslots = j->prog.nslots;
@@ -473,6 +487,8 @@ int admit(nsat_server* s, Job* j) {
 }
 
 void release(nsat_server* s, Job* j) {
+    s->free_slots.push_back(j->slot);
+    j->slot = UINT32_MAX;
     s->arena.release(j->prog_off, prog_bytes(j));
     s->arena.release(j->outs_off, outs_bytes(j));
     if (j->kind == SRV_TABLE) {
@@ -717,6 +733,7 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
         SCK(cudaMalloc(&b.d_vals, kValsCap));
         SCK(cudaMallocHost(&b.h_hdr, sizeof(SrvEpoch)));
         SCK(cudaMallocHost(&b.h_jobs, sizeof(SrvJob) * kMaxActive));
+        SCK(cudaMallocHost(&b.h_state, sizeof(SrvState) * kMaxActive));
         SCK(cudaMallocHost(&b.h_vals, kValsCap));
         memset(b.h_hdr, 0, sizeof(SrvEpoch));
         memset(b.h_jobs, 0, sizeof(SrvJob) * kMaxActive);
@@ -727,6 +744,11 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     SCK(cudaStreamCreateWithFlags(&s->cap2, cudaStreamNonBlocking));
     SCK(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
     SCK(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
+    SCK(cudaMalloc(&s->d_state, sizeof(SrvState) * kMaxActive));
+    SCK(cudaMallocHost(&s->h_state_init, sizeof(SrvState)));
+    memset(s->h_state_init, 0, sizeof(SrvState));
+    s->h_state_init->min_idx = ~0ull;
+    for (uint32_t k = kMaxActive; k-- > 0;) s->free_slots.push_back(k);
     SCK(cudaMalloc(&s->d_join, sizeof(NsatJoinState)));
     SCK(cudaMallocHost(&s->h_join, sizeof(NsatJoinState)));
     // defaults measured on the config-4 trace: 30 ms and 8 workers took a
@@ -827,6 +849,7 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
         if (j->finished) continue;
         if (s->opts.tier_wait && j->tier.load() == TIER_COMPILING) continue;   // compile first
         const uint64_t lim = std::min<uint64_t>(j->total_tiles, j->stop_at);
+        j->sched = std::max(j->sched, j->cursor);     // the device may have rolled over past the plan
         if (j->sched >= lim) continue;
         uint64_t want = std::min<uint64_t>(j->slice, lim - j->sched);
         const uint64_t cost_per_tile = std::max<uint64_t>(1, j->prog.ins.size());
@@ -836,10 +859,11 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
         SrvJob& r = j->rec;
         r.tile_begin = j->sched;
         r.tile_end = j->sched + want;
-        r.claim = r.tile_begin;
-        r.count = 0;
-        r.min_idx = ~0ull;
-        r.any = 0;
+        // SAT and SATOSTOP jobs may go on into the next quarter slice when
+        // warps run out of planned work; QSAT jobs keep exact slices (their
+        // tile values land at planned offsets, and tiering hands blocks over
+        // at planned boundaries)
+        r.tile_hard = j->kind == SRV_QSAT ? r.tile_end : std::min<uint64_t>(lim, r.tile_end + std::max<uint64_t>(1, want / 4));
         r.val_off = (uint32_t)vals;
         if (j->kind == SRV_QSAT && j->qr) vals += want;
         budget -= std::min<uint64_t>(budget, want * cost_per_tile);
@@ -850,7 +874,7 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
         else narrow = std::max(narrow, sl);
         sel[c].push_back(j);
         recs[c].push_back(r);
-        j->sched += want;
+        j->sched = r.tile_hard;      // the furthest the device may claim
         j->slice = std::min<uint64_t>(j->slice * 2, s->opts.max_slice_tiles);
         j->inflight++;
     }
@@ -890,7 +914,7 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
     b.launched = true;
     s->launches += wide ? 2 : 1;
     s->h2d_bytes += sizeof(SrvEpoch) + sizeof(SrvJob) * kMaxActive;   // the graph's copies
-    s->d2h_bytes += sizeof(SrvJob) * kMaxActive + kValsCap;
+    s->d2h_bytes += sizeof(SrvState) * kMaxActive + kValsCap;
     return NSAT_OK;
 }
 
@@ -905,19 +929,22 @@ int process_epoch(nsat_server* s, EpochBuf& b) {
     b.launched = false;
     for (size_t i = 0; i < b.jobs.size(); i++) {
         Job* j = b.jobs[i];
-        const SrvJob& r = b.h_jobs[i];
+        const SrvJob& r = b.h_jobs[i];              // the slice as launched
+        const SrvState& st = b.h_state[j->slot];   // cursor and results as the epoch left them
         j->inflight--;
         if (j->finished) continue;   // answered by an earlier epoch; this slice ran ahead
-        const uint64_t got = r.tile_end - r.tile_begin;
+        // every tile below the device cursor has been evaluated: the kernels
+        // of this and earlier epochs finished before the state was copied
+        const uint64_t got = st.claim - j->cursor;
         j->res.tiles += got;
-        j->cursor = r.tile_end;
+        j->cursor = st.claim;
         bool finished = false;
         if (j->kind == SRV_SAT) {
-            j->count += r.count;
-            if (r.min_idx != ~0ull && !j->res.satisfiable) {
-                // every lower tile was in this or an earlier processed epoch
+            j->count = st.count;
+            if (st.min_idx != ~0ull && !j->res.satisfiable) {
+                // the lowest witness among tiles below the cursor, hence the lowest of all
                 j->res.satisfiable = 1;
-                j->res.witness_lo = r.min_idx >> j->d;
+                j->res.witness_lo = st.min_idx >> j->d;
                 if (!j->find_all) finished = true;
             }
             if (j->cursor == j->total_tiles) finished = true;
@@ -926,15 +953,16 @@ int process_epoch(nsat_server* s, EpochBuf& b) {
             j->res.reversed = j->quants[0];
             j->res.solution_bits = j->f;
             if (!j->qr) {
-                if (r.min_idx != ~0ull) {
+                if (st.min_idx != ~0ull) {
                     j->res.has_solution = 1;
-                    j->res.solution = reverse_bits(r.min_idx, j->f);
+                    j->res.solution = reverse_bits(st.min_idx, j->f);
                     finished = true;
                 } else if (j->cursor == j->total_tiles) {
                     finished = true;
                 }
             } else {
-                for (uint64_t t = 0; t < got && !finished; t++) {
+                // QSAT slices are exact (no roll-over): the slice's tiles, in order
+                for (uint64_t t = 0; t < r.tile_end - r.tile_begin && !finished; t++) {
                     j->qr->push(b.h_vals[r.val_off + t] != 0);
                     FinalResult fr;
                     if (j->qr->final_result(&fr)) {
@@ -946,7 +974,7 @@ int process_epoch(nsat_server* s, EpochBuf& b) {
             }
             if (finished) j->res.value = j->res.has_solution ? (j->quants[0] ? 0 : 1) : (j->quants[0] ? 1 : 0);
         } else {
-            j->any_stop |= r.any != 0;
+            j->any_stop |= st.any != 0;
             if (j->cursor == j->total_tiles) {
                 if (int rc = run_joins(s, j)) return rc;
                 finished = true;

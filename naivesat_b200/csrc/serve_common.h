@@ -57,14 +57,30 @@ struct SrvEpoch {
 };
 #define SRV_NARROW_SLOTS 48
 
-// Device job record; 256 bytes.  Static fields are written at admission,
-// the slice fields every epoch, the result fields by the kernels.
+// A job's search cursor and results, in device memory from admission to
+// release (one entry of the server's state array): the kernel claims tiles
+// by advancing `claim` and accumulates the results here, so they persist
+// across epochs without the host.  64 bytes.
 typedef unsigned long long srv_u64;   // the device atomics' 64-bit type
+
+struct SrvState {
+    srv_u64 claim;              // next tile to hand out; only grows, never past the epoch's limit
+    srv_u64 count;              // SAT: satisfying assignments in the tiles evaluated so far
+    srv_u64 min_idx;            // SAT: lowest witness so far; QSAT (m < tile bits): lowest decisive unit
+    uint32_t any;                // TABLE: some state has STOP
+    uint32_t pad;
+    srv_u64 reserved[4];
+};
+static_assert(sizeof(SrvState) == 64, "SrvState layout");
+
+// Device job record of one epoch; 256 bytes.  Static fields are written at
+// admission, the slice fields every epoch.
+#define SRV_JOB_FIND_ALL 1u      // flags: a SAT job that counts every solution (no early stop)
 
 struct SrvJob {
     // static
     const SrvIns* prog;          // ngroups * G instructions (G: the server shape's group size)
-    const void* unused0;
+    SrvState* st;                // the job's persistent cursor and results
     const uint16_t* outs;        // output slots (bit 15 = negated), nout of them
     srv_u64* table;             // TABLE: 2^np u64 entries (next|STOP<<n | 1<<32)
     uint32_t ngroups;
@@ -77,18 +93,14 @@ struct SrvJob {
     uint32_t n;                  // TABLE: state bits
     srv_u64 allbits;            // QSAT: enumeration bit j has quantifier All
     int8_t in_slot[SRV_MAX_NB];  // enumeration bit -> input slot (-1: dummy)
-    // per epoch
-    srv_u64 tile_begin, tile_end;   // slice of tiles to evaluate
-    uint32_t val_off;                // QSAT: offset of this slice's tile values in the epoch buffer
-    uint32_t pad0;
-    // claimed by the kernel
-    srv_u64 claim;              // next tile (starts at tile_begin)
-    // results
-    srv_u64 count;              // SAT: satisfying assignments in evaluated tiles
-    srv_u64 min_idx;            // SAT: lowest witness; QSAT (m < tile bits): lowest decisive unit
-    uint32_t any;                // TABLE: some state has STOP
-    uint32_t pad1;
-    srv_u64 reserved[10];
+    // per epoch: tiles below tile_end are handed out first; once a warp finds
+    // every job's slice used up it may go on to tile_hard (the next slice,
+    // without a host round trip), unless the job has already been decided
+    srv_u64 tile_begin, tile_end;   // the planned slice
+    srv_u64 tile_hard;               // roll-over limit (== tile_end: none)
+    uint32_t val_off;                // QSAT: offset of the slice's tile values in the epoch buffer
+    uint32_t flags;                  // SRV_JOB_FIND_ALL
+    srv_u64 reserved[13];
 };
 
 static_assert(sizeof(SrvJob) == 256, "SrvJob layout");

@@ -340,7 +340,7 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
                     for (u32 l = 0; l < lanes; l++) dst[l] = (srv_u64)o[l] | (1ull << 32);
                 }
             }
-            if (__any_sync(0xffffffffu, stop_any != 0u) && lane == 0) atomicOr(&J->any, 1u);
+            if (__any_sync(0xffffffffu, stop_any != 0u) && lane == 0) atomicOr(&J->st->any, 1u);
         }
     }
     if (kind == SRV_SAT) {
@@ -349,17 +349,17 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
         idx = warp_min(idx);
         cnt = __reduce_add_sync(0xffffffffu, cnt);
         if (lane == 0 && cnt) {
-            atomicAdd(&J->count, (u64)cnt);
-            atomicMin(&J->min_idx, idx);
+            atomicAdd(&J->st->count, (u64)cnt);
+            atomicMin(&J->st->min_idx, idx);
         }
     } else if (kind == SRV_QSAT) {
         if (M < 10) {
             cand = warp_min(cand);
-            if (lane == 0 && cand != ~0ull) atomicMin(&J->min_idx, cand);
+            if (lane == 0 && cand != ~0ull) atomicMin(&J->st->min_idx, cand);
         } else if (M < SRV_TILE_BITS) {
             const u32 y = tree_rt(acc, allbits, 10, (int)M - 10);
             const u32 d = (dec_all ? ~y : y) & unit_mask((int)M - 10);
-            if (lane == 0 && d != 0u) atomicMin(&J->min_idx, (tile_base >> M) + ((__ffs(d) - 1) >> (M - 10)));
+            if (lane == 0 && d != 0u) atomicMin(&J->st->min_idx, (tile_base >> M) + ((__ffs(d) - 1) >> (M - 10)));
         } else {
             const u32 y = tree_rt(acc, allbits, 10, 5);
             if (lane == 0) vals[J->val_off + (tile - J->tile_begin)] = (uint8_t)(y & 1u);
@@ -368,7 +368,21 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
     __syncwarp();
 }
 
-// One warp per CTA; the dynamic shared memory is max_slots * SRV_SLOT_BYTES.
+// Hands out the job's next tile if it lies below `limit` (~0 otherwise).  A
+// compare-and-swap, so the cursor never passes the limit and stays exact
+// across epochs; a failed swap means another warp took a tile, so the loop
+// ends after at most limit - cursor rounds.
+__device__ __forceinline__ u64 claim_tile(SrvState* st, u64 limit) {
+    u64 cur = *(volatile const u64*)&st->claim;
+    while (cur < limit) {
+        const u64 prev = atomicCAS(&st->claim, cur, cur + 1);
+        if (prev == cur) return cur;
+        cur = prev;
+    }
+    return ~0ull;
+}
+
+// One warp per CTA; the dynamic shared memory is max_slots * slot bytes.
 // cls 0 serves the epoch's narrow jobs, cls 1 its wide ones.
 template <int W, int G, bool DISPATCH>
 __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict__ hdr, SrvJob* __restrict__ jobs,
@@ -384,12 +398,27 @@ __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict_
     dc.sb = hdr->slot_bytes;
     u32 j = njobs ? blockIdx.x % njobs : 0;
     u32 dry = 0;     // consecutive jobs found exhausted
-    while (dry < njobs) {
+    u32 phase = 0;   // 0: the planned slices; 1: on into the next slices
+    for (;;) {
+        if (dry >= njobs) {
+            if (phase == 1) break;
+            phase = 1;
+            dry = 0;
+            if (njobs == 0) break;
+        }
         SrvJob* J = jobs + j;
-        u64 tile = 0;
-        if (lane == 0) tile = atomicAdd(&J->claim, 1ull);
+        u64 tile = ~0ull;
+        if (lane == 0) {
+            u64 lim = phase ? J->tile_hard : J->tile_end;
+            // a decided job (lowest witness or decisive unit found) takes no
+            // tiles beyond its planned slice
+            if (phase && !(J->flags & SRV_JOB_FIND_ALL) && J->kind != SRV_TABLE &&
+                *(volatile const u64*)&J->st->min_idx != ~0ull)
+                lim = J->tile_end;
+            tile = claim_tile(J->st, lim);
+        }
         tile = __shfl_sync(0xffffffffu, tile, 0);
-        if (tile >= J->tile_end) {
+        if (tile == ~0ull) {
             dry++;
             j = (j + 1 == njobs) ? 0 : j + 1;
             continue;
