@@ -804,7 +804,9 @@ def run_serving(args, world, rank, local):
 
     # interpreter work: tiles x LUTs x 1024 words per tile (padding NOPs not counted)
     shape = st_sat["shape"]
-    luts = [api.server_program_check(r["circ"], r["kind"], shape=shape)[1] for r in reqs]
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:    # the ABI call releases the GIL
+        luts = list(pool.map(lambda r: api.server_program_check(r["circ"], r["kind"], shape=shape)[1], reqs))
     words = sum(res_sat[i]["tiles"] * 1024 * luts[i] for i in res_sat)
     lut_words = words / (st_sat["device_ms"] * 1e-3)
     # every LUT-word reads three slot words and writes one in shared memory:

@@ -14,6 +14,7 @@ literals and the test helpers `str_to_quants`/`str_to_bools`) and writes:
   quant_reducer.json        qsat.rs:2036-2466  test_quant_reducer
   aggr_tree_cpu.json        qsat.rs:2629-2835  test_aggr_output_cpu_code
   aggr_tree_opencl.json     qsat.rs:3434-3520  test_aggr_output_opencl_code
+  aggr_tree_cpu_words.json  qsat.rs:2837-3292  test_aggr_output_cpu_code_2
   final_result_circuit.json qsat.rs:6033-6267  final_result_with_circuit
   opencl_quant_reducer.json qsat.rs:4038-6008  test_opencl_quant_reducer
   cpu_outputs_final_result.json qsat.rs:3859-4036
@@ -447,6 +448,19 @@ def main():
                                  "note": "item i = bit (i % 32) of word i // 32; result = full "
                                          "quantifier tree over all items",
                                  "cases": cases}
+
+    body, line = fn_body(qsat, "test_aggr_output_cpu_code_2")
+    cases = []
+    for (elem_bits, quants, tests) in parse_cases(body):
+        for (data, mword, found, result) in tests:
+            cases.append({"elem_bits": elem_bits, "quants": quants, "data": data, "mword": mword,
+                          "found": found, "result": bool(result)})
+    out["aggr_tree_cpu_words.json"] = {
+        "source": "src/qsat.rs:%d test_aggr_output_cpu_code_2" % line,
+        "note": "identity circuit over data: item k = bit k%32 of data[k/32], 2^elem_bits items, 64-bit "
+                "machine words (TYPE_LEN 64); result = the call's value over the last elem_bits quantifiers; "
+                "found = index of the first deciding machine word (not bit-reversed), mword its value",
+        "cases": cases}
 
     body, line = fn_body(qsat, "test_aggr_output_opencl_code")
     cases = []
