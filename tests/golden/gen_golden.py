@@ -15,6 +15,7 @@ literals and the test helpers `str_to_quants`/`str_to_bools`) and writes:
   aggr_tree_cpu.json        qsat.rs:2629-2835  test_aggr_output_cpu_code
   aggr_tree_opencl.json     qsat.rs:3434-3520  test_aggr_output_opencl_code
   aggr_tree_cpu_words.json  qsat.rs:2837-3292  test_aggr_output_cpu_code_2
+  aggr_tree_opencl_groups.json qsat.rs:3522-3857 test_aggr_output_opencl_code_2
   final_result_circuit.json qsat.rs:6033-6267  final_result_with_circuit
   opencl_quant_reducer.json qsat.rs:4038-6008  test_opencl_quant_reducer
   cpu_outputs_final_result.json qsat.rs:3859-4036
@@ -460,6 +461,20 @@ def main():
         "note": "identity circuit over data: item k = bit k%32 of data[k/32], 2^elem_bits items, 64-bit "
                 "machine words (TYPE_LEN 64); result = the call's value over the last elem_bits quantifiers; "
                 "found = index of the first deciding machine word (not bit-reversed), mword its value",
+        "cases": cases}
+
+    body, line = fn_body(qsat, "test_aggr_output_opencl_code_2")
+    cases = []
+    for (quants, group_len, reduce_len, tests) in parse_cases(body):
+        for (data, results) in tests:
+            cases.append({"quants": quants, "group_len": group_len, "reduce_len": reduce_len, "data": data,
+                          "results": [[bool(r), l] for (r, l) in results]})
+    out["aggr_tree_opencl_groups.json"] = {
+        "source": "src/qsat.rs:%d test_aggr_output_opencl_code_2" % line,
+        "note": "identity circuit over data: each of reduce_len groups is group_len 32-lane words (item k of a "
+                "group = bit k%32 of its word k/32) under the last log2(group_len)+5 quantifiers; results: per "
+                "group the value and the local index of the first decisive unit's word (0x7fff none, null "
+                "unchecked)",
         "cases": cases}
 
     body, line = fn_body(qsat, "test_aggr_output_opencl_code")
