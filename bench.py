@@ -558,7 +558,7 @@ def run_ours(args, world, rank, local):
     ms_step = tot_dev / steps
     value = wl.work() * steps / (tot_dev * 1e-3)
     e2e = wl.work() * steps / (tot_e2e * 1e-3)
-    cold = cold_probe(args, local) if world == 1 else None
+    cold = cold_probe(args, local) if (world == 1 and not args.no_e2e_cold) else None
     if cold is not None:
         cold["value"] = wl.work() / (cold["solve_ms"] * 1e-3)
         cold["unit"] = wl.metric
@@ -713,8 +713,12 @@ def run_serving(args, world, rank, local):
     warm = W.serving_requests(64, seed=99, rate_hz=1e9)
     # the interpreter's shape and epoch budget for this GPU (persisted in the
     # kernel cache; servers created with the defaults use them)
-    tune = api.server_tune(ctx, persist=True, retune=True)
-    srv_kw = dict()
+    if args.shape:
+        tune = {"shape": args.shape, "note": "given on the command line, not tuned"}
+        srv_kw = dict(shape=args.shape)
+    else:
+        tune = api.server_tune(ctx, persist=True, retune=True)
+        srv_kw = dict()
 
     peak_lop3, probe_mhz = ctx.lop3_peak()
     srv = api.Server(ctx, **srv_kw)
@@ -876,6 +880,8 @@ def main():
     ap.add_argument("--plain-seconds", type=float, default=60.0, help="c4: time given to the plain form")
     ap.add_argument("--low-rate", type=float, default=2.0, help="c4: a rate the plain form sustains")
     ap.add_argument("--low-seconds", type=float, default=45.0, help="c4: length of the low-rate trace")
+    ap.add_argument("--no-e2e-cold", action="store_true", help="skip the cold-start (new process) solve")
+    ap.add_argument("--shape", type=int, default=0, help="c4: interpreter shape 1..6 instead of tuning one")
     ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
