@@ -11,6 +11,7 @@
 #include "lutmap.h"
 
 #include <algorithm>
+#include <cmath>
 
 namespace nsat {
 
@@ -404,6 +405,25 @@ LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_p
     for (uint32_t i = 0; i < n; i++) if (need[i]) net.used_inputs.push_back(i);
     for (uint32_t j : which) net.outs.push_back(c.outputs[j]);
     return net;
+}
+
+LutNet map_luts_for(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, double log2_space,
+                    double lut_words_per_s) {
+    LutNet net = map_luts(c, which, one_per_gate, 3);
+    if (one_per_gate) return net;
+    // measured on the 3000-gate random DAGs of seeds 1-3: mapping time per
+    // gate, and LUTs relative to three leaves, for 3..6 leaves
+    static const double map_s_per_gate[4] = {1.0e-6, 2.7e-6, 5.5e-6, 9.0e-6};
+    static const double ratio[4] = {1.0, 0.985, 0.965, 0.95};
+    const double words = std::ldexp(1.0, (int)std::max(0.0, log2_space - 5.0));
+    const double search_s = words * (double)net.luts.size() / lut_words_per_s;
+    int best = 3;
+    double best_s = search_s;
+    for (int ke = 4; ke <= KE; ke++) {
+        const double t = map_s_per_gate[ke - 3] * (double)c.gates.size() + search_s * ratio[ke - 3];
+        if (t < best_s) { best_s = t; best = ke; }
+    }
+    return best == 3 ? net : map_luts(c, which, one_per_gate, best);
 }
 
 void eval_lutnet32(const LutNet& net, uint32_t nwires, const uint32_t* inputs, uint32_t* outs) {

@@ -32,12 +32,19 @@ struct LutNet {
 // Maps the cone of outputs `which` (indices into c.outputs).  With
 // one_per_gate, every live gate becomes its own 2-leaf LUT (no fusion).
 // cut_leaves (3..6) bounds the cuts enumerated before support reduction:
-// wider finds smaller covers and costs more time (3000 gates: about 2, 10
-// and 35 ms at 3, 4 and 6).
-constexpr int kCutLeavesCompiled = 6;   // compiled kernels: NVRTC costs far more than mapping
-constexpr int kCutLeavesServed = 4;     // serving programs: mapped per request on builder threads
-LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate,
-                int cut_leaves = kCutLeavesCompiled);
+// wider finds smaller covers and costs more time.  On the 3000-gate random
+// DAGs of the benchmarks, three leaves take about 3 ms and six about 27 ms
+// for 4-6 % fewer LUTs.
+LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves);
+
+// The cover for a search of 2^log2_space assignments evaluated at about
+// `lut_words_per_s`: maps with three leaves, estimates the search's time from
+// that cover, and maps again with wider cuts only when the expected saving
+// beats the extra mapping time (the width minimising mapping plus search).
+LutNet map_luts_for(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, double log2_space,
+                    double lut_words_per_s);
+constexpr double kCompiledLutWordsPerS = 1.85e13;   // compiled kernels: the lop3 issue rate of a B200
+constexpr double kServedLutWordsPerS = 2.0e12;      // the serving interpreter
 
 // Reference evaluation of a LutNet on 32-lane words (used by host self-checks).
 void eval_lutnet32(const LutNet& net, uint32_t nwires, const uint32_t* inputs, uint32_t* outs);

@@ -158,7 +158,8 @@ const LutNet& get_net(nsat_circuit* c, const std::vector<uint32_t>& which) {
     const std::string key = net_key(c, which);
     auto it = c->nets.find(key);
     if (it != c->nets.end()) return it->second;
-    return c->nets[key] = map_luts(c->circ, which, c->ctx->opts.no_optimize != 0);
+    return c->nets[key] = map_luts_for(c->circ, which, c->ctx->opts.no_optimize != 0, c->circ.n,
+                                       kCompiledLutWordsPerS);
 }
 
 // The shape a solve uses: the circuit's tuned one when set, else the
@@ -1135,7 +1136,7 @@ extern "C" int nsat_jit_check(const nsat_circuit_desc* desc, const uint8_t* quan
         which.clear();
         for (uint32_t j = 0; j < c.outputs.size(); j++) which.push_back(j);
     }
-    LutNet net = map_luts(c, which, raw);
+    LutNet net = map_luts_for(c, which, raw, c.n, kCompiledLutWordsPerS);
     std::string err;
     int rc;
     if (kind == 0) {
