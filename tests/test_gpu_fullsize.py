@@ -6,6 +6,11 @@ size-independent properties of the CUDA path's answers.
   the circuit on the CPU, it carries the planted block, and nothing below it
   is a solution (an empty device range up to its 1024-aligned floor, then
   the oracle over the last <= 1023 assignments).
+- config 1 and its unplanted twin, all 2^36 assignments: the exact count and
+  lowest witness equal those of the generated-code CPU path
+  (oracle/cpu_codegen.py, itself pinned to the oracle's interpreter), an
+  independent evaluator fast enough for the whole space (seconds on the
+  host's cores).
 - the 32-bit-state SATOSTOP scale-up (2^32 u64 entries): sampled table
   entries equal the oracle's next state and STOP, and the answer of the
   doubling is a start with its known bits zero whose run stops.
@@ -17,6 +22,19 @@ from naivesat_b200 import workloads as W
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["c1", "c1_twin"])
+def test_full_count_matches_generated_cpu_path(ctx, name):
+    from oracle import cpu_codegen as CG
+    c = W.config(name)
+    full = ctx.circuit(c).sat(find_all=True)
+    g = CG.CodegenSat(c, 24)
+    try:
+        cnt, low = g.sat_args(0, 1 << (c.n - g.e))
+    finally:
+        g.close()
+    assert (full["count"], full["witness"]) == (cnt, low), (name, full, cnt, low)
 
 
 def test_config1_full_enumeration(ctx):
