@@ -372,7 +372,10 @@ int plan_qsat(uint32_t n, const std::vector<uint8_t>& quants_in, bool data, uint
     const uint32_t block_threads = sh.block_threads, min_blocks = sh.min_blocks;
     if (quants_in.size() != n || n == 0) { *err = "quantifier count differs from inputs"; return NSAT_EINVAL; }
     if (prefix_bits >= n) { *err = "prefix must leave at least one free input"; return NSAT_EINVAL; }
-    const uint32_t d = n < 15 ? 15 - n : 0;
+    // dummy innermost inputs (the opposite quantifier of the last one: no
+    // effect on value or witness) for circuits of fewer than 15 inputs, and
+    // for sub-problems that leave fewer than 10 inputs below the prefix
+    const uint32_t d = std::max<uint32_t>(n < 15 ? 15 - n : 0, n - prefix_bits < 10 ? 10 - (n - prefix_bits) : 0);
     const uint32_t np = n + d;
     if (np > 128) { *err = "too many inputs"; return NSAT_EUNSUPPORTED; }
     std::vector<uint8_t> q = quants_in;

@@ -1298,8 +1298,10 @@ extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts,
             return NSAT_OK;
         }
     }
-    // the calibration set: random DAGs of the serving generator, 18-28
-    // inputs (the larger ones carry the work) and 100-4000 gates, log-uniform
+    // the calibration set: random DAGs of the serving generator, 24-30
+    // inputs and 100-4000 gates (log-uniform), large enough that the
+    // interpreter, not the epochs' fixed costs, takes the time (about
+    // 1e11 LUT-words in all)
     const uint32_t njobs = o.jobs ? o.jobs : 24;
     uint64_t st = o.seed ? o.seed : 0x5E7E5E7Eull;
     auto rnd = [&st]() {
@@ -1312,7 +1314,7 @@ extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts,
     std::vector<CalJob> jobs(njobs);
     for (uint32_t i = 0; i < njobs; i++) {
         CalJob& j = jobs[i];
-        j.n = 18 + (uint32_t)(rnd() % 11);
+        j.n = 24 + (uint32_t)(rnd() % 7);
         const double u = (double)(rnd() >> 11) / (double)(1ull << 53);
         const uint32_t g = (uint32_t)std::exp(std::log(100.0) + u * (std::log(4000.0) - std::log(100.0)));
         j.gates.assign(3 * g, 0);
@@ -1347,8 +1349,9 @@ extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts,
         if (int rc = serve_calibration(ctx, jobs, res->shape, budgets[b], &lw, &dms, &wms, &ep)) return rc;
         res->budget_solves_per_s[b] = wms > 0 ? njobs / (wms * 1e-3) : 0;
         res->budget_epoch_ms[b] = ep ? wms / (double)ep : 0;
-        if (res->budget_epoch_ms[b] <= 20.0 && res->budget_solves_per_s[b] > best_rate) {
-            best_rate = res->budget_solves_per_s[b];
+        // the larger budget unless it is slower by more than the noise (2 %)
+        if (res->budget_epoch_ms[b] <= 20.0 && res->budget_solves_per_s[b] > 0.98 * best_rate) {
+            best_rate = std::max(best_rate, res->budget_solves_per_s[b]);
             res->epoch_budget = budgets[b];
         }
     }
