@@ -70,10 +70,28 @@ class ClockSampler:
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
                                       "--format=csv,noheader,nounits", "-lms", "200"],
                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        # a region shorter than the sampling period still gets a sample on
+        # each side: wait for the first one before the region starts
+        self.lines_at_start = self._wait_lines(1, 5.0)
+
+    def _wait_lines(self, n, limit_s):
+        t0 = time.time()
+        while time.time() - t0 < limit_s:
+            self.f.flush()
+            try:
+                with open(self.path) as f:
+                    k = sum(1 for _ in f)
+            except OSError:
+                k = 0
+            if k >= n:
+                return k
+            time.sleep(0.02)
+        return 0
 
     def stop(self):
         if not self.proc:
             return None
+        self._wait_lines(self.lines_at_start + 1, 1.0)     # and one after it ends
         self.proc.terminate()
         try:
             self.proc.wait(5)
