@@ -123,6 +123,21 @@ struct Mapper {
 
     explicit Mapper(const Circuit& cc) : c(cc), n(cc.n), W(cc.wires()) {}
 
+    // The per-node arrays live in buffers kept per host thread between
+    // calls: a fresh allocation of several hundred KB per mapping costs more
+    // in page faults than the mapping of a small circuit itself.
+    struct Buffers {
+        std::vector<uint8_t> live, ncut, nwide;
+        std::vector<uint32_t> fanout;
+        std::vector<Cut> cuts, wide, best;
+        std::vector<float> af;
+        std::vector<int32_t> refs;
+    };
+    void swap_buffers(Buffers& b) {
+        live.swap(b.live); ncut.swap(b.ncut); nwide.swap(b.nwide); fanout.swap(b.fanout);
+        cuts.swap(b.cuts); wide.swap(b.wide); best.swap(b.best); af.swap(b.af); refs.swap(b.refs);
+    }
+
     bool is_gate(uint32_t w) const { return w >= n; }
     const Gate& gate(uint32_t w) const { return c.gates[w - n]; }
     const Cut* cuts_of(uint32_t w) const { return &cuts[(size_t)(w - n) * P]; }
@@ -220,7 +235,7 @@ struct Mapper {
     void enumerate() {
         cuts.assign((size_t)(W - n) * P, Cut());
         ncut.assign(W - n, 0);
-        wide.assign((size_t)(W - n) * Q, Cut());
+        if (ke > K) wide.assign((size_t)(W - n) * Q, Cut());   // no wider cuts to keep at K leaves
         nwide.assign(W - n, 0);
         best.assign(W, Cut());
         af.assign(W, 0.f);
@@ -312,6 +327,12 @@ struct ConeEval {
 LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves) {
     LutNet net;
     Mapper m(c);
+    static thread_local Mapper::Buffers buffers;
+    struct Keep {
+        Mapper& m;
+        ~Keep() { m.swap_buffers(buffers); }
+    } keep{m};
+    m.swap_buffers(buffers);
     m.ke = std::max(K, std::min(KE, cut_leaves));
     const uint32_t n = c.n, W = c.wires();
     m.live.assign(W, 0);
