@@ -212,7 +212,9 @@ def test_continuous_batching_jobs_arrive_while_others_run(ctx):
         if k == 4:
             time.sleep(0.05)
             a, q = step()
-            assert q > 0, "SATOSTOP jobs beyond the arena must wait in the queue"
+            st = srv.stats()
+            assert q > 0, ("SATOSTOP jobs beyond the arena must wait in the queue", st,
+                           {t: (res[t]["status"], res[t]["admit_ms"], res[t]["done_ms"]) for t in wait_tags if t in res})
     for x in srv.run_all():
         res[x["tag"]] = x
     srv.close()
