@@ -737,6 +737,8 @@ def run_serving(args, world, rank, local):
     else:
         tune = api.server_tune(ctx, persist=True, retune=True)
         srv_kw = dict()
+    if args.epoch_budget:
+        srv_kw["epoch_budget"] = args.epoch_budget
 
     peak_lop3, probe_mhz = ctx.lop3_peak()
     srv = api.Server(ctx, **srv_kw)
@@ -768,6 +770,22 @@ def run_serving(args, world, rank, local):
         kp = len(service)
         prefix = reqs[:kp]
         wres, wservice = serving.plain_service_times(ctx, prefix, 1e9, cache_dir=cache_dir)
+        # the server with the same warm kernel cache (its QSAT tiering finds
+        # the kernels compiled): the like-for-like partner of the warm form
+        old_cache = os.environ.get("NSAT_JIT_CACHE")
+        os.environ["NSAT_JIT_CACHE"] = cache_dir
+        try:
+            srv = api.Server(ctx, **srv_kw)
+            wbres, wblat, wbmk = serving.replay_server(srv, prefix, realtime=False)
+            srv.close()
+            srv = api.Server(ctx, **srv_kw)
+            wpres, wplat, wpmk = serving.replay_server(srv, prefix, realtime=True)
+            srv.close()
+        finally:
+            if old_cache is None:
+                os.environ.pop("NSAT_JIT_CACHE", None)
+            else:
+                os.environ["NSAT_JIT_CACHE"] = old_cache
     finally:
         shutil.rmtree(cache_dir, ignore_errors=True)
     srv = api.Server(ctx, **srv_kw)
@@ -783,13 +801,17 @@ def run_serving(args, world, rank, local):
     same = 0
     for i in range(kp):
         v = serving.verdict(reqs[i]["kind"], res_sat[i])
-        forms = (pres[i], wres[i], ires[i], bres[i], pres_b[i])
+        forms = (pres[i], wres[i], ires[i], bres[i], pres_b[i], wbres[i], wpres[i])
         assert all(serving.verdict(reqs[i]["kind"], f) == v for f in forms), i
         same += 1
     arr = [r["arrival_s"] for r in prefix]
     server_prefix = serving.summarize(plat_b, pmk_b, kp)
     server_prefix["solves_per_s"] = kp / bmk
     server_prefix["note"] = "solves/s with the requests queued at t=0; latencies under the Poisson arrivals"
+    server_warm = serving.summarize(wplat, wpmk, kp)
+    server_warm["solves_per_s"] = kp / wbmk
+    server_warm["note"] = ("the same with the warm kernel cache of the compiled_warm_cache form (QSAT tiering "
+                           "loads its kernels instead of compiling them)")
 
     def one_at_a_time(svc, form):
         lat = serving.fifo_latencies(arr, svc)
@@ -800,9 +822,10 @@ def run_serving(args, world, rank, local):
                 "service_p50_ms": serving.percentile(svc, 50) * 1e3,
                 "service_p99_ms": serving.percentile(svc, 99) * 1e3,
                 "server_speedup": server_prefix["solves_per_s"] / sps,
+                "warm_server_speedup": server_warm["solves_per_s"] / sps,
                 "keeps_up_at_rate": sps > args.rate}
     plain_forms = {
-        "requests": kp, "rate_hz": args.rate, "server": server_prefix,
+        "requests": kp, "rate_hz": args.rate, "server": server_prefix, "server_warm_cache": server_warm,
         "interpreter_alone": one_at_a_time(iservice, "the precompiled interpreter, one job per server at a "
                                                      "time (same server options, no batching)"),
         "compiled_warm_cache": one_at_a_time(wservice, "one-shot solvers with every kernel already in the "
@@ -900,6 +923,7 @@ def main():
     ap.add_argument("--low-seconds", type=float, default=45.0, help="c4: length of the low-rate trace")
     ap.add_argument("--no-e2e-cold", action="store_true", help="skip the cold-start (new process) solve")
     ap.add_argument("--shape", type=int, default=0, help="c4: interpreter shape 1..6 instead of tuning one")
+    ap.add_argument("--epoch-budget", type=int, default=0, help="c4: epoch budget instead of the tuned one")
     ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
