@@ -407,9 +407,9 @@ typedef struct {
  * evaluated, so the work is fixed: 24-30 inputs, 100-4000 gates) under every
  * interpreter shape and keeps the one with the most LUT-words per second of
  * device time; then, for that shape, times the same set with epoch budgets of
- * 1.2e7 .. 9.6e7 and keeps the largest whose throughput is within 2 % of the
- * best and whose mean epoch stays under 20 ms (longer epochs delay
- * arrivals).  With `persist` the
+ * 1.2e7 .. 9.6e7.  The set measures throughput, not the latency of arrivals,
+ * so the default budget (4.8e7) stays unless another is more than 5 % faster
+ * with a mean epoch under 20 ms.  With `persist` the
  * choice is written to the kernel cache directory, keyed by GPU, and servers
  * created later with shape 0 and epoch_budget 0 use it; an existing choice is
  * read back instead of timing again unless `retune` is set. */

@@ -1339,22 +1339,24 @@ extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts,
             res->shape = sh;
         }
     }
-    // the epoch budget for that shape, by wall clock, under the epoch-length cap
+    // the epoch budget for that shape, by wall clock.  The calibration set
+    // measures throughput, not the latency of arrivals, so the default (4.8e7,
+    // the best p99 and solves/s on the config-4 trace) stays unless another
+    // budget is clearly faster (5 %) with epochs under 20 ms.
     static const uint64_t budgets[4] = {12000000, 24000000, 48000000, 96000000};
-    double best_rate = -1;
-    res->epoch_budget = 48000000;
+    const int kDefault = 2;
     for (int b = 0; b < 4; b++) {
         double lw = 0, dms = 0, wms = 0;
         uint64_t ep = 0;
         if (int rc = serve_calibration(ctx, jobs, res->shape, budgets[b], &lw, &dms, &wms, &ep)) return rc;
         res->budget_solves_per_s[b] = wms > 0 ? njobs / (wms * 1e-3) : 0;
         res->budget_epoch_ms[b] = ep ? wms / (double)ep : 0;
-        // the larger budget unless it is slower by more than the noise (2 %)
-        if (res->budget_epoch_ms[b] <= 20.0 && res->budget_solves_per_s[b] > 0.98 * best_rate) {
-            best_rate = std::max(best_rate, res->budget_solves_per_s[b]);
-            res->epoch_budget = budgets[b];
-        }
     }
+    int pick = kDefault;
+    for (int b = 0; b < 4; b++)
+        if (res->budget_epoch_ms[b] <= 20.0 && res->budget_solves_per_s[b] > 1.05 * res->budget_solves_per_s[pick])
+            pick = b;
+    res->epoch_budget = budgets[pick];
     if (o.persist) {
         jit_cache_dir_created();
         const std::string path = tuned_path(ctx), tmp = path + ".tmp";
