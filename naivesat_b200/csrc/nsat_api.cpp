@@ -182,10 +182,16 @@ void choose_shape(uint32_t C, uint32_t block_threads, KernelConfig* kc, uint32_t
     }
     if (wb > C - 10) wb = C - 10;
     uint32_t rest = C - 10 - wb;
-    // small launches keep 8 iterations per warp (down to 2^8 CTAs): one
-    // word per thread in 2048 CTAs left c0 (2^24 assignments) launch-bound,
-    // 13.6 us against 8.7 us with 256 CTAs of more iterations
-    uint32_t cb = std::min<uint32_t>(rest, std::min<uint32_t>(cb_max ? cb_max : 12, std::max<uint32_t>(8, rest - 3)));
+    // small launches keep 4 iterations per warp while the grid still holds
+    // 2^12 warps (one wave at 24 resident warps per SM): one word per thread
+    // in 2048 CTAs left c0 (2^24 assignments) launch-bound at 13.6 us, 256
+    // CTAs of 8 warps latency-bound at 12.8 us, 4096 warps of 4 iterations
+    // took 8.7 us
+    const uint32_t cap = cb_max ? cb_max : 12;
+    const uint32_t wave = wb < 12 ? 12 - wb : 0;       // CTA bits for 2^12 warps
+    uint32_t cb = std::min<uint32_t>(rest, cap);
+    if (rest >= 2) cb = std::min<uint32_t>(cb, rest - 2);
+    cb = std::max<uint32_t>(cb, std::min<uint32_t>(rest, std::min<uint32_t>(wave, cap)));
     uint32_t it = rest - cb;
     if (it > 10) { it = 10; cb = rest - 10; }
     kc->wb = wb; kc->it = it; kc->cb = cb; kc->c = C;

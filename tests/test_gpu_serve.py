@@ -171,7 +171,9 @@ def test_continuous_batching_jobs_arrive_while_others_run(ctx):
     epochs as the long ones, and that the memory waiters were admitted only
     after an earlier table was released."""
     import time
-    longs = [{"kind": "sat", "circ": W.random_dag(800 + s, 30, 500, output="live"), "quants": None,
+    # about 1200 LUTs over 2^32 assignments each: over 100 ms of interpreter
+    # time in slices that double per epoch, so they run through the whole test
+    longs = [{"kind": "sat", "circ": W.random_dag(820 + s, 32, 3000, output="live"), "quants": None,
               "unknowns": 0, "find_all": True} for s in range(2)]
     qc = W.random_dag(810, 29, 400, output="live")
     longs.append({"kind": "qsat", "circ": qc, "quants": "A" * 13 + "E" * 16, "unknowns": 0})
