@@ -865,6 +865,16 @@ def run_serving(args, world, rank, local):
     kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("sat", "qsat", "stop")}
     sat_sum = serving.summarize(lat_sat, mk_sat, len(res_sat))
     poi_sum = serving.summarize(lat_poi, mk_poi, len(res_poi))
+    # where the tail comes from: percentiles per kind, and for the QSAT jobs
+    # that raced a compiled kernel
+    keys = sorted(res_poi)
+    groups = {}
+    for k, lat in zip(keys, lat_poi):
+        groups.setdefault(reqs[k]["kind"], []).append(lat)
+        if res_poi[k]["compiled_blocks"]:
+            groups.setdefault("qsat_tiered", []).append(lat)
+    poi_sum["by_kind"] = {g: {"requests": len(v), "p50_ms": serving.percentile(v, 50) * 1e3,
+                              "p99_ms": serving.percentile(v, 99) * 1e3} for g, v in groups.items()}
     line = {
         "metric": "solves/s", "value": sat_sum["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
         "steps": len(reqs), "warmup": len(warm), "ms_per_step": 1e3 / sat_sum["solves_per_s"],
