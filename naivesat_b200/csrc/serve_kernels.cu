@@ -26,9 +26,12 @@
 // computes.
 //
 // Scheduling is on the device: every warp starts at its own job of the epoch
-// table and claims tiles of that job's slice with an atomic cursor, moving on
-// round-robin when a slice is used up; a warp ends after one full pass finds
-// nothing left (no waiting on anything).
+// table and claims tiles from the job's persistent cursor, moving on
+// round-robin when the job's slice is used up.  The search for the next job
+// with tiles left checks 32 jobs at a time, one per lane.  When no slice has
+// planned tiles left, warps go on into the next quarter slice of SAT and
+// SATOSTOP jobs that are not decided yet, and end when none has tiles left
+// either (no waiting on anything).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -368,6 +371,16 @@ __device__ __forceinline__ void do_tile(SrvJob* J, u64 tile, char* __restrict__ 
     __syncwarp();
 }
 
+// The tile a job may hand out up to: its planned slice, or in the roll-over
+// phase its next quarter slice, unless it has been decided already (lowest
+// witness or decisive unit found).
+__device__ __forceinline__ u64 claim_limit(const SrvJob* J, u32 phase) {
+    if (!phase) return J->tile_end;
+    if (!(J->flags & SRV_JOB_FIND_ALL) && J->kind != SRV_TABLE && *(volatile const u64*)&J->st->min_idx != ~0ull)
+        return J->tile_end;
+    return J->tile_hard;
+}
+
 // Hands out the job's next tile if it lies below `limit` (~0 otherwise).  A
 // compare-and-swap, so the cursor never passes the limit and stays exact
 // across epochs; a failed swap means another warp took a tile, so the loop
@@ -397,33 +410,35 @@ __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict_
     dc.km = hdr->hi_mul;
     dc.sb = hdr->slot_bytes;
     u32 j = njobs ? blockIdx.x % njobs : 0;
-    u32 dry = 0;     // consecutive jobs found exhausted
     u32 phase = 0;   // 0: the planned slices; 1: on into the next slices
-    for (;;) {
-        if (dry >= njobs) {
+    while (njobs) {
+        // the first job at or after j (round robin) with a tile left below
+        // its limit: 32 jobs per step, one per lane, so a pass over an epoch
+        // of hundreds of jobs costs a few dependent L2 reads, not hundreds
+        int pick = -1;
+        for (u32 base = 0; base < njobs && pick < 0; base += 32) {
+            const u32 k = base + lane;
+            bool has = false;
+            u32 jj = 0;
+            if (k < njobs) {
+                jj = j + k;
+                if (jj >= njobs) jj -= njobs;
+                has = *(volatile const u64*)&jobs[jj].st->claim < claim_limit(&jobs[jj], phase);
+            }
+            const u32 m = __ballot_sync(0xffffffffu, has);
+            if (m) pick = __shfl_sync(0xffffffffu, (int)jj, __ffs(m) - 1);
+        }
+        if (pick < 0) {
             if (phase == 1) break;
             phase = 1;
-            dry = 0;
-            if (njobs == 0) break;
-        }
-        SrvJob* J = jobs + j;
-        u64 tile = ~0ull;
-        if (lane == 0) {
-            u64 lim = phase ? J->tile_hard : J->tile_end;
-            // a decided job (lowest witness or decisive unit found) takes no
-            // tiles beyond its planned slice
-            if (phase && !(J->flags & SRV_JOB_FIND_ALL) && J->kind != SRV_TABLE &&
-                *(volatile const u64*)&J->st->min_idx != ~0ull)
-                lim = J->tile_end;
-            tile = claim_tile(J->st, lim);
-        }
-        tile = __shfl_sync(0xffffffffu, tile, 0);
-        if (tile == ~0ull) {
-            dry++;
-            j = (j + 1 == njobs) ? 0 : j + 1;
             continue;
         }
-        dry = 0;
+        SrvJob* J = jobs + pick;
+        u64 tile = ~0ull;
+        if (lane == 0) tile = claim_tile(J->st, claim_limit(J, phase));
+        tile = __shfl_sync(0xffffffffu, tile, 0);
+        j = (u32)pick;   // stay on this job while it has tiles
+        if (tile == ~0ull) continue;   // another warp took the last one
         do_tile<W, G, DISPATCH>(J, tile, Sl, lane, vals, dc);
     }
 }
