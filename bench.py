@@ -739,6 +739,8 @@ def run_serving(args, world, rank, local):
         srv_kw = dict()
     if args.epoch_budget:
         srv_kw["epoch_budget"] = args.epoch_budget
+    if args.rollover:
+        srv_kw["rollover"] = True
 
     peak_lop3, probe_mhz = ctx.lop3_peak()
     srv = api.Server(ctx, **srv_kw)
@@ -934,6 +936,7 @@ def main():
     ap.add_argument("--no-e2e-cold", action="store_true", help="skip the cold-start (new process) solve")
     ap.add_argument("--shape", type=int, default=0, help="c4: interpreter shape 1..6 instead of tuning one")
     ap.add_argument("--epoch-budget", type=int, default=0, help="c4: epoch budget instead of the tuned one")
+    ap.add_argument("--rollover", action="store_true", help="c4: servers with roll-over into the next slices")
     ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()

@@ -341,7 +341,9 @@ typedef struct {
                                    every block runs compiled (compile first instead of racing) */
     uint32_t shape;             /* interpreter shape, 1..NSAT_SERVE_SHAPES (below); 0 = the shape
                                    nsat_server_tune persisted for this GPU, else the default */
-    uint32_t reserved;
+    uint32_t rollover;          /* 1: warps that run out of planned work go on into the next
+                                   quarter slice of undecided SAT and SATOSTOP jobs, with no host
+                                   round trip; 0: each epoch evaluates exactly its slices */
 } nsat_server_opts;
 
 /* Interpreter shapes: words per lane W (W x 1024 assignments per warp and

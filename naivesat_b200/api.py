@@ -112,7 +112,7 @@ class ServerOpts(C.Structure):
                 ("max_slice_tiles", C.c_uint32), ("first_slice_tiles", C.c_uint32),
                 ("epoch_budget", C.c_uint64), ("build_threads", C.c_uint32), ("tier_threads", C.c_uint32),
                 ("tier_min_ms", C.c_uint32), ("tier_wait", C.c_uint32), ("shape", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("rollover", C.c_uint32)]
 
 
 class ServeTuneOpts(C.Structure):
@@ -443,12 +443,13 @@ class Server:
 
     def __init__(self, ctx, arena_bytes=0, max_active=0, max_queue=0, max_slice_tiles=0,
                  first_slice_tiles=0, epoch_budget=0, build_threads=0, tier_threads=0, tier_min_ms=0,
-                 tier_wait=False, shape=0):
+                 tier_wait=False, shape=0, rollover=False):
         """shape: interpreter shape 1..SERVE_SHAPES (include/nsat.h), 0 = the
         one tuned for this GPU (nsat_server_tune) or the default."""
         self.ctx = ctx
         o = ServerOpts(arena_bytes, max_active, max_queue, max_slice_tiles, first_slice_tiles, epoch_budget,
-                       build_threads, tier_threads, tier_min_ms, 1 if tier_wait else 0, shape, 0)
+                       build_threads, tier_threads, tier_min_ms, 1 if tier_wait else 0, shape,
+                       1 if rollover else 0)
         h = C.c_void_p()
         ctx._check(lib().nsat_server_create(ctx.h, C.byref(o), C.byref(h)), "server_create")
         self.h = h

@@ -863,7 +863,9 @@ int launch_epoch(nsat_server* s, EpochBuf& b) {
         // warps run out of planned work; QSAT jobs keep exact slices (their
         // tile values land at planned offsets, and tiering hands blocks over
         // at planned boundaries)
-        r.tile_hard = j->kind == SRV_QSAT ? r.tile_end : std::min<uint64_t>(lim, r.tile_end + std::max<uint64_t>(1, want / 4));
+        r.tile_hard = (j->kind == SRV_QSAT || !s->opts.rollover)
+                          ? r.tile_end
+                          : std::min<uint64_t>(lim, r.tile_end + std::max<uint64_t>(1, want / 4));
         r.val_off = (uint32_t)vals;
         if (j->kind == SRV_QSAT && j->qr) vals += want;
         budget -= std::min<uint64_t>(budget, want * cost_per_tile);

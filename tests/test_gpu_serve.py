@@ -293,3 +293,23 @@ def test_server_tune_persists_and_is_used(ctx, tmp_path, monkeypatch):
     srv = api.Server(ctx)
     assert srv.stats()["shape"] == t["shape"]
     srv.close()
+
+
+def test_rollover_matches_oracle(ctx):
+    """With roll-over on, warps that run out of planned work claim the next
+    quarter slice of undecided SAT and SATOSTOP jobs from the device cursors;
+    every answer still equals the oracle's (counts included for count-mode
+    jobs, so no tile is evaluated twice or skipped)."""
+    reqs = small_mix(36, 67)
+    srv = api.Server(ctx, rollover=True, tier_min_ms=0xFFFFFFFF)
+    for i, r in enumerate(reqs):
+        srv.submit(r["kind"], r["circ"], quants=r["quants"], unknowns=r["unknowns"], tag=i,
+                   find_all=(r["kind"] == "sat" and i % 2 == 0))
+    res = {r["tag"]: r for r in srv.run_all()}
+    srv.close()
+    for i, r in enumerate(reqs):
+        exp = expected(r)
+        assert project(res[i], exp) == exp, (i, r["kind"], res[i], exp)
+        if r["kind"] == "sat" and i % 2 == 0:
+            c = r["circ"]
+            assert res[i]["count"] == O.sat_range(O.Circuit(c.n, c.gates, c.outputs))[0], i
