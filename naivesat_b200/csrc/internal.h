@@ -3,6 +3,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 
 #include "nsat.h"
@@ -32,6 +33,14 @@ Circuit circuit_from_desc(const nsat_circuit_desc* d);
 int qsat_solve_with_scratch(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants,
                             const nsat_qsat_opts* opts, nsat_qsat_result* res,
                             unsigned char* scratch, size_t scratch_bytes);
+
+// The QSAT sub-problems under prefixes first .. first + count - 1 of
+// prefix_bits fixed inputs, solved back to back through the launch ring when
+// each is one launch (otherwise only count == 1 is accepted); on_block sees
+// each result in prefix order and returns false to stop.
+int qsat_solve_blocks(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants, uint32_t prefix_bits,
+                      uint64_t first, uint64_t count,
+                      const std::function<bool(uint64_t, const nsat_qsat_result&)>& on_block);
 
 // Next-state entries (next | STOP << n, u64) of states first_state ..
 // first_state+count-1 (both multiples of 32) into device memory dev_out, on

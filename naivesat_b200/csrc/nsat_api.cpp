@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <atomic>
 #include <thread>
 #include <chrono>
@@ -713,10 +714,16 @@ extern "C" int nsat_sat_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_sat_opt
 
 namespace {
 
+// With prefix_count > 1 (one launch per prefix only), solves the sub-problems
+// under prefixes prefix .. prefix + prefix_count - 1 back to back through the
+// launch ring and hands each one's result, in order, to on_block, which
+// returns false to stop; res then holds the last one handed over.
 int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quants_in,
                 const uint32_t* data_words, uint32_t n_items_bits, uint32_t chunk_bits,
                 nsat_qsat_result* res, unsigned char* fixed_scratch = nullptr,
-                size_t fixed_scratch_bytes = 0, uint32_t prefix_bits = 0, uint64_t prefix = 0) {
+                size_t fixed_scratch_bytes = 0, uint32_t prefix_bits = 0, uint64_t prefix = 0,
+                uint64_t prefix_count = 1,
+                const std::function<bool(uint64_t, const nsat_qsat_result&)>* on_block = nullptr) {
     memset(res, 0, sizeof(*res));
     const double t_start = now_ms();
     if (int rc = set_device(ctx)) return rc;
@@ -771,13 +778,15 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
         CK(cudaMemcpyAsync(ctx->d_data, ex.data(), nw * 4, cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     }
+    if (prefix_count > 1 && (A != 0 || !on_block || (prefix_bits < 64 && prefix + prefix_count > (1ull << prefix_bits))))
+        return fail(ctx, NSAT_EUNSUPPORTED, "a run of prefixes needs one launch per prefix");
     const bool q0all = q[s] != 0;
     const bool dec = !q0all;   // value of a decisive unit
     std::unique_ptr<QuantReducer> qr;
     if (A > 0) qr.reset(new QuantReducer(std::vector<uint8_t>(q.begin() + s, q.begin() + s + A)));
     FinalResult fr;
     bool have = false;
-    uint64_t nl = A == 64 ? ~0ull : (1ull << A);
+    uint64_t nl = prefix_count > 1 ? prefix_count : (A == 64 ? ~0ull : (1ull << A));
     const unsigned grid = 1u << kc.cb, threads = kc.threads();
     uint64_t launch_idx_buf[kRing];
     LaunchOut* d_out = ctx->d_out;
@@ -800,6 +809,15 @@ int qsat_common(nsat_ctx* ctx, nsat_circuit* c, const std::vector<uint8_t>& quan
                 fr.has_solution = r.min_idx != ~0ull;
                 fr.solution = fr.has_solution ? reverse_bits(r.min_idx, f) : 0;
                 have = true;
+                if (prefix_count > 1) {
+                    nsat_qsat_result b{};
+                    b.reversed = fr.reversed;
+                    b.solution_bits = fr.solution_bits;
+                    b.has_solution = fr.has_solution;
+                    b.value = fr.has_solution ? (q0all ? 0 : 1) : (q0all ? 1 : 0);
+                    b.solution_lo = fr.solution;
+                    return (*on_block)(prefix + k, b);
+                }
                 return false;
             }
             bool value;
@@ -850,6 +868,21 @@ extern "C" int nsat_qsat_solve(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* qu
     if (f > 64) return fail(ctx, NSAT_EUNSUPPORTED, "first quantifier block longer than 64");
     return qsat_common(ctx, c, q, nullptr, 0, opts ? opts->chunk_bits : 0, res, nullptr, 0,
                        opts ? opts->prefix_bits : 0, opts ? opts->prefix : 0);
+}
+
+int nsat::qsat_solve_blocks(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quants, uint32_t prefix_bits,
+                            uint64_t first, uint64_t count,
+                            const std::function<bool(uint64_t, const nsat_qsat_result&)>& on_block) {
+    if (!ctx || !c || !quants || count == 0) return NSAT_EINVAL;
+    std::vector<uint8_t> q(quants, quants + c->circ.n);
+    for (auto& v : q) v = v ? 1 : 0;
+    nsat_qsat_result last{};
+    if (count == 1) {
+        int rc = qsat_common(ctx, c, q, nullptr, 0, 0, &last, nullptr, 0, prefix_bits, first);
+        if (rc == NSAT_OK) on_block(first, last);
+        return rc;
+    }
+    return qsat_common(ctx, c, q, nullptr, 0, 0, &last, nullptr, 0, prefix_bits, first, count, &on_block);
 }
 
 int nsat::ctx_device(const nsat_ctx* ctx) { return ctx ? ctx->device : -1; }

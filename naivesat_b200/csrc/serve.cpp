@@ -653,15 +653,33 @@ void tier_loop(nsat_server* s, nsat_opts copts) {
         }
         if (from >= 0 && !j->tier_cancel && !s->tstop) {
             j->tier = TIER_RUNNING;
-            for (uint64_t p = (uint64_t)from; p + 1 < nblocks; p++) {
-                if (j->tier_cancel || s->tstop) break;
-                nsat_qsat_result r{};
-                if (solve(p, &r) != NSAT_OK) {
-                    j->tier_rc = NSAT_ECUDA;
-                    break;
+            // the remaining blocks back to back: their launches queue on the
+            // worker's stream at once, so they fill the gaps between
+            // interpreter epochs instead of taking one gap each
+            const uint64_t first = (uint64_t)from, count = nblocks - 1 - first;
+            auto post = [&](uint64_t p, const nsat_qsat_result& r) {
+                {
+                    std::lock_guard<std::mutex> lk(j->tmu);
+                    j->blk[p] = r;
                 }
-                std::lock_guard<std::mutex> lk(j->tmu);
-                j->blk[p] = r;
+                return !(j->tier_cancel || s->tstop);
+            };
+            if (count > 0) {
+                int brc = qsat_solve_blocks(wctx, cw, j->quants.data(), sbits, first, count, post);
+                if (brc == NSAT_EUNSUPPORTED) {
+                    // blocks of several launches each: one solve per block
+                    for (uint64_t p = first; p + 1 < nblocks; p++) {
+                        if (j->tier_cancel || s->tstop) break;
+                        nsat_qsat_result r{};
+                        if (solve(p, &r) != NSAT_OK) {
+                            j->tier_rc = NSAT_ECUDA;
+                            break;
+                        }
+                        post(p, r);
+                    }
+                } else if (brc != NSAT_OK) {
+                    j->tier_rc = NSAT_ECUDA;
+                }
             }
         }
         nsat_circuit_free(cw);
