@@ -245,7 +245,11 @@ def test_continuous_batching_jobs_arrive_while_others_run(ctx):
                      find_all=r.get("find_all", False))
         got = alone.run_all()[0]
         alone.close()
-        keys = ("count", "satisfiable", "witness") if r["kind"] == "sat" else \
+        # a find-mode SAT job's count covers the slices processed before its
+        # first solution was seen, which depends on the epochs it shared, so
+        # counts are compared for full-count jobs only
+        sat_keys = ("count", "satisfiable", "witness") if r.get("find_all") else ("satisfiable", "witness")
+        keys = sat_keys if r["kind"] == "sat" else \
             ("reversed", "solution_bits", "solution") if r["kind"] == "qsat" else ("found", "start", "end", "steps")
         assert {k: got[k] for k in keys} == {k: res[i][k] for k in keys}, (i, got, res[i])
 
