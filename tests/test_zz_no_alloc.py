@@ -4,15 +4,17 @@ allocator or a fixed budget, where cudaMalloc/cudaFree would synchronize the
 device or overrun the budget mid-request).  Its scratch is the library's
 static device array, so its answers must equal the allocating
 nsat_qsat_solve's, bit for bit, call after call (the array keeps the previous
-call's bytes).  This file is collected last on purpose."""
+call's bytes), and the oracle's where the oracle finishes in seconds.  This file is collected last on purpose."""
 import pytest
 
 from naivesat_b200 import api
 from naivesat_b200 import workloads as W
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
 KEYS = ("reversed", "solution_bits", "solution", "value")
+ORACLE_KEYS = ("reversed", "solution_bits", "solution")
 
 
 def cases():
@@ -27,14 +29,27 @@ def cases():
     yield adder, "E" * 16 + "A" * 16, 0
 
 
+def oracle_answer(circ, quants):
+    """The oracle's FinalResult where it finishes in seconds (24 inputs), the
+    adder's known counterexample (a = 0, 16 bits, reversed) otherwise."""
+    if circ.n <= 24:
+        return O.qsat(O.Circuit(circ.n, circ.gates, circ.outputs), quants, mode=1)
+    if quants == circ.quants:
+        return {"reversed": True, "solution_bits": 16, "solution": 0}
+    return None
+
+
 def test_noalloc_matches_allocating_solve_twice():
     with api.Context(0) as ctx:
         for circ, quants, chunk in cases():
             h = ctx.circuit(circ)
             ref = h.qsat(quants, chunk_bits=chunk)
+            exp = oracle_answer(circ, quants)
             for call in range(2):
                 got = h.qsat_noalloc(quants, chunk_bits=chunk)
                 assert {k: got[k] for k in KEYS} == {k: ref[k] for k in KEYS}, (circ.name, quants, call)
+                if exp is not None:
+                    assert {k: got[k] for k in ORACLE_KEYS} == exp, (circ.name, quants, call)
 
 
 def test_noalloc_boundary_launch_of_2_15_ctas():
