@@ -741,6 +741,8 @@ def run_serving(args, world, rank, local):
         srv_kw["epoch_budget"] = args.epoch_budget
     if args.rollover:
         srv_kw["rollover"] = True
+    if args.max_slice_tiles:
+        srv_kw["max_slice_tiles"] = args.max_slice_tiles
 
     peak_lop3, probe_mhz = ctx.lop3_peak()
     srv = api.Server(ctx, **srv_kw)
@@ -887,6 +889,7 @@ def run_serving(args, world, rank, local):
                                "at t=0 (value) and with Poisson arrivals at %.0f/s (latency)"
                                % (len(reqs), kinds["sat"], kinds["qsat"], kinds["stop"], args.rate),
                    "step": "one request solved", "epochs": st_sat["epochs"],
+                   "server_options": {k: (bool(v) if k == "rollover" else v) for k, v in srv_kw.items()},
                    "qsat_tiering": {"jobs": sum(1 for r in res_sat.values() if r["compiled_blocks"]),
                                     "compiled_blocks": sum(r["compiled_blocks"] for r in res_sat.values()),
                                     "note": "large QSAT jobs race a kernel compiled for them; its 1/16 prefix "
@@ -937,6 +940,7 @@ def main():
     ap.add_argument("--shape", type=int, default=0, help="c4: interpreter shape 1..6 instead of tuning one")
     ap.add_argument("--epoch-budget", type=int, default=0, help="c4: epoch budget instead of the tuned one")
     ap.add_argument("--rollover", action="store_true", help="c4: servers with roll-over into the next slices")
+    ap.add_argument("--max-slice-tiles", type=int, default=0, help="c4: largest slice of a job per epoch (tiles)")
     ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()

@@ -412,33 +412,37 @@ __global__ void __launch_bounds__(32, 1) serve_epoch(const SrvEpoch* __restrict_
     u32 j = njobs ? blockIdx.x % njobs : 0;
     u32 phase = 0;   // 0: the planned slices; 1: on into the next slices
     while (njobs) {
-        // the first job at or after j (round robin) with a tile left below
-        // its limit: 32 jobs per step, one per lane, so a pass over an epoch
-        // of hundreds of jobs costs a few dependent L2 reads, not hundreds
-        int pick = -1;
-        for (u32 base = 0; base < njobs && pick < 0; base += 32) {
-            const u32 k = base + lane;
-            bool has = false;
-            u32 jj = 0;
-            if (k < njobs) {
-                jj = j + k;
-                if (jj >= njobs) jj -= njobs;
-                has = *(volatile const u64*)&jobs[jj].st->claim < claim_limit(&jobs[jj], phase);
-            }
-            const u32 m = __ballot_sync(0xffffffffu, has);
-            if (m) pick = __shfl_sync(0xffffffffu, (int)jj, __ffs(m) - 1);
-        }
-        if (pick < 0) {
-            if (phase == 1) break;
-            phase = 1;
-            continue;
-        }
-        SrvJob* J = jobs + pick;
+        // the job this warp is on: one claim, no search
+        SrvJob* J = jobs + j;
         u64 tile = ~0ull;
         if (lane == 0) tile = claim_tile(J->st, claim_limit(J, phase));
         tile = __shfl_sync(0xffffffffu, tile, 0);
-        j = (u32)pick;   // stay on this job while it has tiles
-        if (tile == ~0ull) continue;   // another warp took the last one
+        if (tile == ~0ull) {
+            // the next job after j (round robin) with a tile left below its
+            // limit: 32 jobs per step, one per lane, so a pass over an epoch
+            // of hundreds of jobs costs a few dependent L2 reads, not hundreds
+            int pick = -1;
+            for (u32 base = 1; base < njobs && pick < 0; base += 32) {
+                const u32 k = base + lane;
+                bool has = false;
+                u32 jj = 0;
+                if (k < njobs) {
+                    jj = j + k;
+                    if (jj >= njobs) jj -= njobs;
+                    has = *(volatile const u64*)&jobs[jj].st->claim < claim_limit(&jobs[jj], phase);
+                }
+                const u32 m = __ballot_sync(0xffffffffu, has);
+                if (m) pick = __shfl_sync(0xffffffffu, (int)jj, __ffs(m) - 1);
+            }
+            if (pick >= 0) {
+                j = (u32)pick;   // claimed on the next turn (or found dry there)
+            } else if (phase == 0) {
+                phase = 1;       // job j itself is tried again at the new limit
+            } else {
+                break;
+            }
+            continue;
+        }
         do_tile<W, G, DISPATCH>(J, tile, Sl, lane, vals, dc);
     }
 }
