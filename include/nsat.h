@@ -326,9 +326,9 @@ typedef struct {
     uint32_t max_slice_tiles;   /* cap of one job's tiles per epoch; 0 = 4096 */
     uint32_t first_slice_tiles; /* a new job's first slice (doubling after); 0 = 1 */
     uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = the
-                                   budget nsat_server_tune persisted for this GPU, else 4.8e7
-                                   (on the config-4 trace smaller budgets raised p99 and lowered
-                                   solves/s) */
+                                   budget nsat_server_tune persisted for this GPU, else 1.2e7
+                                   (on a mixed serving trace: the most solves/s, the same p99
+                                   as 6e6-4.8e7) */
     uint32_t build_threads;     /* host threads that build job programs; 0 = min(8, cores / 2) */
     uint32_t tier_threads;      /* QSAT tiering workers (own context each); 0 = three quarters of
                                    the host threads, between 2 and 12 */
@@ -410,7 +410,7 @@ typedef struct {
  * interpreter shape and keeps the one with the most LUT-words per second of
  * device time; then, for that shape, times the same set with epoch budgets of
  * 1.2e7 .. 9.6e7.  The set measures throughput, not the latency of arrivals,
- * so the default budget (4.8e7) stays unless another is more than 5 % faster
+ * so the default budget (1.2e7) stays unless another is more than 5 % faster
  * with a mean epoch under 20 ms.  With `persist` the
  * choice is written to the kernel cache directory, keyed by GPU, and servers
  * created later with shape 0 and epoch_budget 0 use it; an existing choice is
@@ -428,7 +428,7 @@ typedef struct {
     uint32_t from_cache;                           /* read back, nothing timed */
     uint64_t epoch_budget;                         /* chosen */
     double lut_words_per_s[NSAT_SERVE_SHAPES];     /* per shape, device time (0 = not timed) */
-    double budget_solves_per_s[4];                 /* budgets 1.2e7, 2.4e7, 4.8e7, 9.6e7: wall clock */
+    double budget_solves_per_s[4];                 /* budgets 6e6, 1.2e7, 2.4e7, 4.8e7: wall clock */
     double budget_epoch_ms[4];                     /* their mean epoch wall time */
     double tune_ms;
 } nsat_serve_tune_result;

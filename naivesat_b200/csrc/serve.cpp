@@ -46,6 +46,7 @@ namespace {
 
 constexpr uint32_t kMaxActive = 512;
 constexpr uint32_t kDefaultShape = 0;        // index into kSrvShapes when nothing was tuned
+constexpr uint64_t kDefaultBudget = 12000000; // epoch budget when nothing was tuned
 constexpr size_t kValsCap = 256 * 1024;      // QSAT tile values per epoch
 constexpr double kInterpRate = 1.5e12;        // interpreter LUT-words/s (measured), for the tiering estimate
 
@@ -739,7 +740,7 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
             if (!s->opts.epoch_budget) s->opts.epoch_budget = budget;
         }
     }
-    if (!s->opts.epoch_budget) s->opts.epoch_budget = 48000000;
+    if (!s->opts.epoch_budget) s->opts.epoch_budget = kDefaultBudget;
     s->shape = s->opts.shape ? s->opts.shape - 1 : kDefaultShape;
     SCK(cudaSetDevice(ctx_device(ctx)));
     SCK(cudaMalloc(&s->arena.base, s->opts.arena_bytes));
@@ -1352,7 +1353,7 @@ extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts,
     for (uint32_t sh = 1; sh <= SRV_NSHAPES; sh++) {
         double lw = 0, dms = 0, wms = 0;
         uint64_t ep = 0;
-        if (int rc = serve_calibration(ctx, jobs, sh, 48000000, &lw, &dms, &wms, &ep)) return rc;
+        if (int rc = serve_calibration(ctx, jobs, sh, kDefaultBudget, &lw, &dms, &wms, &ep)) return rc;
         res->lut_words_per_s[sh - 1] = dms > 0 ? lw / (dms * 1e-3) : 0;
         if (res->lut_words_per_s[sh - 1] > best) {
             best = res->lut_words_per_s[sh - 1];
@@ -1360,11 +1361,13 @@ extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts,
         }
     }
     // the epoch budget for that shape, by wall clock.  The calibration set
-    // measures throughput, not the latency of arrivals, so the default (4.8e7,
-    // the best p99 and solves/s on the config-4 trace) stays unless another
-    // budget is clearly faster (5 %) with epochs under 20 ms.
-    static const uint64_t budgets[4] = {12000000, 24000000, 48000000, 96000000};
-    const int kDefault = 2;
+    // measures throughput, not the latency of arrivals, so the default (1.2e7,
+    // the most solves/s at the same p99 on the mixed SAT/QSAT/SATOSTOP serving
+    // trace) stays unless another budget is clearly faster (5 %) with epochs
+    // under 20 ms.
+    static constexpr uint64_t budgets[4] = {6000000, 12000000, 24000000, 48000000};
+    constexpr int kDefault = 1;
+    static_assert(budgets[kDefault] == kDefaultBudget, "the default budget is a candidate");
     for (int b = 0; b < 4; b++) {
         double lw = 0, dms = 0, wms = 0;
         uint64_t ep = 0;
