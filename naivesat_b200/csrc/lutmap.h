@@ -37,10 +37,17 @@ struct LutNet {
 // for 4-6 % fewer LUTs.
 LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves);
 
+// Gates in the cone of outputs `which`.
+uint32_t live_gate_count(const Circuit& c, const std::vector<uint32_t>& which);
+
 // The cover for a search of 2^log2_space assignments evaluated at about
-// `lut_words_per_s`: maps with three leaves, estimates the search's time from
-// that cover, and maps again with wider cuts only when the expected saving
-// beats the extra mapping time (the width minimising mapping plus search).
+// `lut_words_per_s`.  When even one LUT per live gate would search in under
+// a quarter of the time that cut mapping takes (small index spaces: the
+// 2^24 search of a 500-gate circuit is about 8 us of lop3 work against about
+// 0.3 ms of mapping), the cover is one LUT per gate, a linear pass.
+// Otherwise it maps with three leaves, estimates the search's time from that
+// cover, and maps again with wider cuts only when the expected saving beats
+// the extra mapping time (the width minimising mapping plus search).
 LutNet map_luts_for(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, double log2_space,
                     double lut_words_per_s);
 constexpr double kCompiledLutWordsPerS = 1.85e13;   // compiled kernels: the lop3 issue rate of a B200

@@ -16,6 +16,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "circuit.h"
@@ -66,6 +67,12 @@ struct nsat_ctx {
     size_t data_bytes = 0;
     NsatJoinState* d_join = nullptr;
     NsatJoinState* h_join = nullptr;
+    // loaded kernels by everything their generated source depends on (the
+    // kernel configuration, the entry point and the LUT net, compared
+    // whole): a fresh circuit handle whose cover and launch configuration
+    // were seen before skips generating and hashing the source.  The entries
+    // are weak, so the JIT module cache alone decides what stays loaded.
+    std::unordered_map<std::string, std::pair<CUfunction, std::weak_ptr<JitModule>>> by_inputs;
 };
 
 // Launch shape of the evaluator kernels: threads per CTA, CTAs per SM the
@@ -221,14 +228,56 @@ int ensure_scratch(nsat_ctx* ctx, size_t bytes) {
     return NSAT_OK;
 }
 
+// The inputs of generate_source as one byte string: the configuration key,
+// the entry point and the net's LUTs, inputs and outputs (counts first).
+std::string source_inputs(const KernelConfig& kc, const LutNet& net, const char* name) {
+    std::string k = kc.key();
+    k += '|';
+    k += name;
+    k += '|';
+    auto put = [&k](const void* p, size_t n) { k.append(static_cast<const char*>(p), n); };
+    const uint32_t counts[3] = {(uint32_t)net.luts.size(), (uint32_t)net.used_inputs.size(),
+                                (uint32_t)net.outs.size()};
+    put(counts, sizeof(counts));
+    k.reserve(k.size() + net.luts.size() * 18 + net.used_inputs.size() * 4 + net.outs.size() * 5);
+    for (const Lut& L : net.luts) {
+        put(&L.wire, 4);
+        put(&L.nin, 1);
+        put(L.in, 12);
+        put(&L.tt, 1);
+    }
+    put(net.used_inputs.data(), net.used_inputs.size() * 4);
+    for (const Output& o : net.outs) {
+        const uint8_t neg = o.neg ? 1 : 0;
+        put(&o.wire, 4);
+        put(&neg, 1);
+    }
+    return k;
+}
+
 int get_kernel(nsat_ctx* ctx, const KernelConfig& kc, const LutNet& net, const char* name,
                CUfunction* fn, std::shared_ptr<JitModule>* holder) {
+    std::string key = source_inputs(kc, net, name);
+    auto it = ctx->by_inputs.find(key);
+    if (it != ctx->by_inputs.end()) {
+        if (std::shared_ptr<JitModule> m = it->second.second.lock()) {
+            *fn = it->second.first;
+            *holder = std::move(m);
+            return NSAT_OK;
+        }
+    }
     std::string src = generate_source(kc, net);
     std::string err;
     int rc = jit_get(ctx->device, src, {name}, ctx->opts.verbose != 0, holder, &err);
     if (rc == -3) return fail(ctx, NSAT_ECOMPILE, err);
     if (rc != 0) return fail(ctx, NSAT_ECUDA, err);
     *fn = (*holder)->fns[name];
+    if (ctx->by_inputs.size() >= 1024) {     // drop entries whose modules were evicted
+        for (auto e = ctx->by_inputs.begin(); e != ctx->by_inputs.end();)
+            e = e->second.second.expired() ? ctx->by_inputs.erase(e) : std::next(e);
+        if (ctx->by_inputs.size() >= 1024) ctx->by_inputs.clear();
+    }
+    ctx->by_inputs[std::move(key)] = {*fn, *holder};
     return NSAT_OK;
 }
 

@@ -104,11 +104,12 @@ def test_lut_mapping_saves_ops():
     assert fused["lop3_ops"] < 0.8 * fused["live_gates"], fused
 
 
-@pytest.mark.parametrize("name,kind,lop3", [("c0", "sat", 170), ("c1", "sat", 1229), ("c1_twin", "sat", 1354),
+@pytest.mark.parametrize("name,kind,lop3", [("c0", "sat", 280), ("c1", "sat", 1229), ("c1_twin", "sat", 1354),
                                             ("c2a", "qsat", 38), ("c2c", "qsat", 665)])
 def test_lut_counts_of_the_benchmark_circuits(name, kind, lop3):
     """The mapper is deterministic; these covers are the ones the measured
-    rooflines count."""
+    rooflines count.  c0's 2^24 search is short next to cut mapping, so its
+    cover is one LUT per live gate (280); the others are cut covers."""
     c = W.config(name)
     assert api.jit_check(c, kind, quants=c.quants)["lop3_ops"] == lop3
 
