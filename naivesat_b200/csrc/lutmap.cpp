@@ -443,14 +443,15 @@ LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_p
 }
 
 LutNet map_luts_for(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, double log2_space,
-                    double lut_words_per_s) {
+                    double lut_words_per_s, bool shared_device) {
     if (one_per_gate) return map_luts(c, which, true, 3);
     // measured on the 3000-gate random DAGs of seeds 1-3: mapping time per
     // gate, and LUTs relative to three leaves, for 3..6 leaves
     static const double map_s_per_gate[4] = {1.0e-6, 2.7e-6, 5.5e-6, 9.0e-6};
     static const double ratio[4] = {1.0, 0.985, 0.965, 0.95};
     const double words = std::ldexp(1.0, (int)std::max(0.0, log2_space - 5.0));
-    if (words * (double)live_gate_count(c, which) / lut_words_per_s < 0.25 * map_s_per_gate[0] * (double)c.gates.size())
+    if (!shared_device &&
+        words * (double)live_gate_count(c, which) / lut_words_per_s < 0.25 * map_s_per_gate[0] * (double)c.gates.size())
         return map_luts(c, which, true, 3);
     LutNet net = map_luts(c, which, false, 3);
     const double search_s = words * (double)net.luts.size() / lut_words_per_s;

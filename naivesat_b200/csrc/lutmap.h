@@ -41,15 +41,17 @@ LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_p
 uint32_t live_gate_count(const Circuit& c, const std::vector<uint32_t>& which);
 
 // The cover for a search of 2^log2_space assignments evaluated at about
-// `lut_words_per_s`.  When even one LUT per live gate would search in under
-// a quarter of the time that cut mapping takes (small index spaces: the
-// 2^24 search of a 500-gate circuit is about 8 us of lop3 work against about
-// 0.3 ms of mapping), the cover is one LUT per gate, a linear pass.
+// `lut_words_per_s`.  For a solve that has the device to itself: when even
+// one LUT per live gate would search in under a quarter of the time that cut
+// mapping takes (small index spaces: the 2^24 search of a 500-gate circuit is
+// about 8 us of lop3 work against about 0.3 ms of mapping), the cover is one
+// LUT per gate, a linear pass.  With `shared_device` (jobs of a server, whose
+// device time every other job waits for) that shortcut is not taken.
 // Otherwise it maps with three leaves, estimates the search's time from that
 // cover, and maps again with wider cuts only when the expected saving beats
 // the extra mapping time (the width minimising mapping plus search).
 LutNet map_luts_for(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, double log2_space,
-                    double lut_words_per_s);
+                    double lut_words_per_s, bool shared_device = false);
 constexpr double kCompiledLutWordsPerS = 1.85e13;   // compiled kernels: the lop3 issue rate of a B200
 constexpr double kServedLutWordsPerS = 2.0e12;      // the serving interpreter
 

@@ -112,7 +112,7 @@ struct Program {
 
 bool build_program(const Circuit& c, const std::vector<uint32_t>& which, bool raw, uint32_t group, Program* p,
                    std::string* err) {
-    LutNet net = map_luts_for(c, which, raw, c.n, kServedLutWordsPerS);
+    LutNet net = map_luts_for(c, which, raw, c.n, kServedLutWordsPerS, true);
     const uint32_t W = c.wires();
     const size_t L = net.luts.size();
     std::vector<int32_t> lut_of(W, -1);
@@ -1346,7 +1346,7 @@ extern "C" int nsat_server_tune(nsat_ctx* ctx, const nsat_serve_tune_opts* opts,
         j.gates.resize(3 * gn);
         const nsat_circuit_desc d{j.n, gn, j.gates.data(), 1, j.outs.data()};
         const Circuit c = circuit_from_desc(&d);
-        j.luts = map_luts_for(c, {0}, ctx_no_optimize(ctx), c.n, kServedLutWordsPerS).luts.size();
+        j.luts = map_luts_for(c, {0}, ctx_no_optimize(ctx), c.n, kServedLutWordsPerS, true).luts.size();
     }
     // every shape at the default budget, by device time
     double best = -1;
