@@ -770,10 +770,11 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     for (uint32_t k = kMaxActive; k-- > 0;) s->free_slots.push_back(k);
     SCK(cudaMalloc(&s->d_join, sizeof(NsatJoinState)));
     SCK(cudaMallocHost(&s->h_join, sizeof(NsatJoinState)));
-    // defaults measured on the config-4 trace: 30 ms and 8 workers took a
-    // 3000-request prefix from 366 to 609 solves/s (p99 at 150/s 172 -> 42 ms);
-    // on all 10,000 requests, 12 workers (the compiles are the limit) reach
-    // 517 solves/s against 435 with 8
+    // defaults measured on the 10,000-request mixed serving trace: 30 ms and
+    // 8 workers took its first 3000 requests from 366 to 609 solves/s; on all
+    // of it, 12 workers (the compiles are the limit) reach 517 solves/s
+    // against 435 with 8.  Thresholds of 4-15 ms tier more jobs and lower p99
+    // on some runs, but cost 3-7 % of solves/s on the whole trace.
     if (s->opts.tier_min_ms == 0) s->opts.tier_min_ms = 30;
     const uint32_t hw_tier = std::max(2u, std::min(12u, std::thread::hardware_concurrency() * 3 / 4));
     const uint32_t ntier =
