@@ -627,7 +627,9 @@ def cold_probe(args, local):
     cache: context creation, LUT mapping, source generation, NVRTC compile,
     module load, launches and readback.  Returns its timings (or None)."""
     tmp = tempfile.mkdtemp(prefix="nsat_cold_")
-    env = dict(os.environ, NSAT_JIT_CACHE=tmp)
+    # empty kernel caches: this library's and the CUDA compute cache, where
+    # NVRTC also keeps what it compiled
+    env = dict(os.environ, NSAT_JIT_CACHE=tmp, CUDA_CACHE_PATH=os.path.join(tmp, "cuda"))
     cmd = [sys.executable, os.path.abspath(__file__), "--cold-probe", "--workload", args.workload,
            "--log2", str(args.log2), "--device", str(local)]
     try:
@@ -950,6 +952,19 @@ def main():
     if args.cold_probe:
         run_cold_probe(args)
         return
+    # NVRTC keeps compiled kernels in the CUDA compute cache (CUDA_CACHE_PATH,
+    # by default shared by every process of the user), so a kernel that an
+    # earlier run compiled would make this run's cold figures (e2e_cold, the
+    # empty-cache plain form of c4) warm.  Every run starts from an empty one.
+    cuda_cache = tempfile.mkdtemp(prefix="nsat_cuda_cache_")
+    os.environ["CUDA_CACHE_PATH"] = cuda_cache
+    try:
+        run_main(args)
+    finally:
+        shutil.rmtree(cuda_cache, ignore_errors=True)
+
+
+def run_main(args):
     world, rank, local = dist_setup()
     try:
         if args.workload == "c4":

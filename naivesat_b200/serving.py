@@ -156,7 +156,10 @@ def plain_service_times(ctx, reqs, time_limit_s, fresh_jit_cache=True, cache_dir
     fresh_jit_cache the kernels compile into an empty on-disk cache, as in a
     new process; cache_dir instead names the on-disk cache to use (a second
     pass over the same requests with the same directory finds every kernel
-    compiled: the warm-cache plain form)."""
+    compiled: the warm-cache plain form).  NVRTC also keeps what it compiles
+    in the CUDA compute cache (CUDA_CACHE_PATH), which is read once per
+    process: a caller timing cold compiles points it at an empty directory
+    before the process first uses CUDA, as bench.py does."""
     old = os.environ.get("NSAT_JIT_CACHE")
     tmp = tempfile.TemporaryDirectory(prefix="nsat_plain_") if (fresh_jit_cache and cache_dir is None) else None
     if tmp is not None:
