@@ -66,8 +66,10 @@ bool pwrite_all(int fd, const void* buf, uint64_t len, uint64_t off) {
 // Packed bytes of `count` entries of `bits` bits (count a multiple of 64).
 uint64_t packed_bytes(uint64_t count, uint32_t bits) { return ((count * bits) >> 6) * 8; }
 
-// The image and every buffer the solve uses.
+// The image and every buffer the solve uses.  Device buffers come from the
+// context's stream-ordered pool (ctx_alloc), so a repeated solve reuses them.
 struct Work {
+    nsat_ctx* ctx = nullptr;
     int storage = DEVICE;
     uint64_t bytes = 0;
     uint64_t* dev_image = nullptr;    // DEVICE
@@ -86,14 +88,12 @@ struct Work {
     std::vector<cudaEvent_t> jev;     // a start/end pair per join of one partition step
 
     ~Work() {
-        if (copy) cudaStreamSynchronize(copy);
-        cudaFree(dev_image);
-        cudaFree(dest);
-        cudaFree(snap);
-        cudaFree(stage[0]);
-        cudaFree(stage[1]);
-        cudaFree(chunk);
-        cudaFree(best);
+        if (copy) cudaStreamSynchronize(copy);   // the copy stream's uses end before the frees
+        if (ctx) {
+            for (void* p : {(void*)dev_image, (void*)dest, (void*)snap, (void*)stage[0], (void*)stage[1],
+                            (void*)chunk, (void*)best})
+                ctx_free(ctx, p);
+        }
         if (host_image) cudaFreeHost(host_image);
         if (host_stage) cudaFreeHost(host_stage);
         for (int k = 0; k < 2; k++) {
@@ -136,6 +136,7 @@ int check_opts(nsat_ctx* ctx, uint32_t n, const nsat_greedy_opts* o, uint32_t* p
 // Chooses where the image lives and allocates the image and work buffers.
 int setup(nsat_ctx* ctx, Work& w, uint32_t n, uint64_t L, uint64_t chunk, const nsat_greedy_opts* o,
           bool joins) {
+    w.ctx = ctx;
     const uint32_t P = o->partitions;
     const uint32_t bits = n + 1;
     w.bytes = packed_bytes(1ull << n, bits);
@@ -153,9 +154,9 @@ int setup(nsat_ctx* ctx, Work& w, uint32_t n, uint64_t L, uint64_t chunk, const 
         w.storage = (w.bytes + work_dev <= budget) ? DEVICE : HOST;
     }
     if (w.storage == DEVICE) {
-        GCK(cudaMalloc(&w.dev_image, w.bytes));
+        GCK(ctx_alloc(ctx, (void**)&w.dev_image, w.bytes));
     } else {
-        for (int k = 0; k < 2; k++) GCK(cudaMalloc(&w.stage[k], std::max(pbytes, cbytes)));
+        for (int k = 0; k < 2; k++) GCK(ctx_alloc(ctx, (void**)&w.stage[k], std::max(pbytes, cbytes)));
         if (w.storage == HOST) {
             cudaError_t e = cudaMallocHost(&w.host_image, w.bytes);
             if (e != cudaSuccess) {
@@ -177,12 +178,13 @@ int setup(nsat_ctx* ctx, Work& w, uint32_t n, uint64_t L, uint64_t chunk, const 
             GCK(cudaMallocHost(&w.host_stage, std::max(pbytes, cbytes)));
         }
     }
-    GCK(cudaMalloc(&w.chunk, chunk * 8));
-    GCK(cudaMalloc(&w.best, 8));
+    GCK(ctx_alloc(ctx, (void**)&w.chunk, chunk * 8));
+    GCK(ctx_alloc(ctx, (void**)&w.best, 8));
     if (joins) {
-        GCK(cudaMalloc(&w.dest, L * 8));
-        GCK(cudaMalloc(&w.snap, L * 8));
+        GCK(ctx_alloc(ctx, (void**)&w.dest, L * 8));
+        GCK(ctx_alloc(ctx, (void**)&w.snap, L * 8));
     }
+    GCK(cudaStreamSynchronize(ctx_stream(ctx)));   // the pool's buffers are ready on every stream
     GCK(cudaStreamCreateWithFlags(&w.copy, cudaStreamNonBlocking));
     for (int k = 0; k < 2; k++) {
         GCK(cudaEventCreateWithFlags(&w.ready[k], cudaEventDisableTiming));

@@ -23,6 +23,14 @@ bool ctx_no_optimize(const nsat_ctx* ctx);
 nsat_opts ctx_opts(const nsat_ctx* ctx);
 // Records a failure on the context (nsat_last_error) and returns `code`.
 int ctx_fail(nsat_ctx* ctx, int code, const std::string& msg);
+// Per-call device buffers (tables, partition images, work areas) from the
+// context's stream-ordered pool: allocated and freed in order on the
+// context's stream, and kept for reuse by the next call (up to a release
+// threshold), so a repeated solve pays no cudaMalloc/cudaFree.  A buffer
+// used on another stream needs the context's stream synchronised after the
+// allocation.
+cudaError_t ctx_alloc(nsat_ctx* ctx, void** p, size_t bytes);
+void ctx_free(nsat_ctx* ctx, void* p);
 
 // Circuit from the C ABI's flat description (not validated).
 Circuit circuit_from_desc(const nsat_circuit_desc* d);

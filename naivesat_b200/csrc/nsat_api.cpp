@@ -73,7 +73,12 @@ struct nsat_ctx {
     // were seen before skips generating and hashing the source.  The entries
     // are weak, so the JIT module cache alone decides what stays loaded.
     std::unordered_map<std::string, std::pair<CUfunction, std::weak_ptr<JitModule>>> by_inputs;
+    cudaMemPool_t pool = nullptr;     // per-call buffers (ctx_alloc)
 };
+
+// Memory the context's pool keeps for reuse after its buffers are freed;
+// beyond it the pool returns memory at the next synchronisation.
+constexpr uint64_t kPoolKeepBytes = 8ull << 30;
 
 // Launch shape of the evaluator kernels: threads per CTA, CTAs per SM the
 // kernels are compiled for, and the cap on CTA bits per launch (the rest of
@@ -109,11 +114,11 @@ struct nsat_table {
     int cur = 0;          // buffer holding the current table
     bool any_stop = false;
     double build_ms = 0;
-    ~nsat_table() {
+    ~nsat_table() {       // the buffers came from the context's pool
         if (buf[0] || buf[1]) {
             cudaSetDevice(ctx->device);
-            if (buf[0]) cudaFree(buf[0]);
-            if (buf[1]) cudaFree(buf[1]);
+            nsat::ctx_free(ctx, buf[0]);
+            nsat::ctx_free(ctx, buf[1]);
         }
     }
 };
@@ -542,6 +547,14 @@ extern "C" int nsat_create(int device, const nsat_opts* opts, nsat_ctx** out) {
     CK(cudaFree(nullptr));
     CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = device;
+    CK(cudaMemPoolCreate(&ctx->pool, &pp));
+    uint64_t keep = kPoolKeepBytes;
+    CK(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     CK(cudaMalloc(&ctx->d_out, sizeof(LaunchOut) * kRing));
     CK(cudaMallocHost(&ctx->h_out, sizeof(LaunchOut) * kRing));
     CK(cudaMallocHost(&ctx->h_init, sizeof(LaunchOut)));
@@ -577,6 +590,7 @@ extern "C" void nsat_destroy(nsat_ctx* ctx) {
     cudaFree(ctx->d_join);
     cudaFreeHost(ctx->h_join);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
 }
 
@@ -936,6 +950,12 @@ int nsat::qsat_solve_blocks(nsat_ctx* ctx, nsat_circuit* c, const uint8_t* quant
 
 int nsat::ctx_device(const nsat_ctx* ctx) { return ctx ? ctx->device : -1; }
 cudaStream_t nsat::ctx_stream(const nsat_ctx* ctx) { return ctx->stream; }
+cudaError_t nsat::ctx_alloc(nsat_ctx* ctx, void** p, size_t bytes) {
+    return cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+}
+void nsat::ctx_free(nsat_ctx* ctx, void* p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
+}
 int nsat::ctx_sm_count(const nsat_ctx* ctx) { return ctx->sm_count; }
 bool nsat::ctx_no_optimize(const nsat_ctx* ctx) { return ctx->opts.no_optimize != 0; }
 nsat_opts nsat::ctx_opts(const nsat_ctx* ctx) { return ctx->opts; }
@@ -983,8 +1003,9 @@ extern "C" int nsat_stop_table_build(nsat_ctx* ctx, nsat_circuit* c, const nsat_
     t->entry_bytes = kc.fmt == 0 ? 4 : 8;
     const size_t bytes = std::max<size_t>(t->N * t->entry_bytes, 256);
     for (int i = 0; i < 2; i++) {
-        cudaError_t e = cudaMalloc(&t->buf[i], bytes);
+        cudaError_t e = ctx_alloc(ctx, &t->buf[i], bytes);
         if (e != cudaSuccess) {
+            t->buf[i] = nullptr;
             cudaGetLastError();
             return fail(ctx, NSAT_ENOMEM, "table allocation failed");
         }
