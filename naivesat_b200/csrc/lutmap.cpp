@@ -338,7 +338,8 @@ uint32_t live_gate_count(const Circuit& c, const std::vector<uint32_t>& which) {
     return k;
 }
 
-LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves) {
+LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves,
+                int recovery_passes) {
     LutNet net;
     Mapper m(c);
     static thread_local Mapper::Buffers buffers;
@@ -381,7 +382,7 @@ LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_p
             if (m.is_gate(w) && m.refs[w]++ == 0) m.ref_cut(m.best[w]);
         }
         // exact-area recovery (two passes)
-        for (int pass = 0; pass < 2; pass++) {
+        for (int pass = 0; pass < recovery_passes; pass++) {
             for (uint32_t w = n; w < W; w++) {
                 if (!m.live[w] || m.refs[w] <= 0) continue;
                 m.deref_cut(m.best[w]);
@@ -450,10 +451,15 @@ LutNet map_luts_for(const Circuit& c, const std::vector<uint32_t>& which, bool o
     static const double map_s_per_gate[4] = {1.0e-6, 2.7e-6, 5.5e-6, 9.0e-6};
     static const double ratio[4] = {1.0, 0.985, 0.965, 0.95};
     const double words = std::ldexp(1.0, (int)std::max(0.0, log2_space - 5.0));
-    if (!shared_device &&
-        words * (double)live_gate_count(c, which) / lut_words_per_s < 0.25 * map_s_per_gate[0] * (double)c.gates.size())
+    const double gate_search_s = words * (double)live_gate_count(c, which) / lut_words_per_s;
+    if (!shared_device && gate_search_s < 0.25 * map_s_per_gate[0] * (double)c.gates.size())
         return map_luts(c, which, true, 3);
-    LutNet net = map_luts(c, which, false, 3);
+    // The second exact-area pass costs 20-35 % of the mapping and saved at
+    // most one LUT on the benchmark circuits: it runs only for searches of
+    // 0.1 s and more (estimated from the live gates at 0.6 LUTs per gate),
+    // where its cost stays under about 1 % of the solve.
+    const int passes = 0.6 * gate_search_s >= 0.1 ? 2 : 1;
+    LutNet net = map_luts(c, which, false, 3, passes);
     const double search_s = words * (double)net.luts.size() / lut_words_per_s;
     int best = 3;
     double best_s = search_s;
@@ -461,7 +467,7 @@ LutNet map_luts_for(const Circuit& c, const std::vector<uint32_t>& which, bool o
         const double t = map_s_per_gate[ke - 3] * (double)c.gates.size() + search_s * ratio[ke - 3];
         if (t < best_s) { best_s = t; best = ke; }
     }
-    return best == 3 ? net : map_luts(c, which, one_per_gate, best);
+    return best == 3 ? net : map_luts(c, which, one_per_gate, best, passes);
 }
 
 void eval_lutnet32(const LutNet& net, uint32_t nwires, const uint32_t* inputs, uint32_t* outs) {

@@ -31,11 +31,14 @@ struct LutNet {
 
 // Maps the cone of outputs `which` (indices into c.outputs).  With
 // one_per_gate, every live gate becomes its own 2-leaf LUT (no fusion).
+// recovery_passes: exact-area recovery passes over the cover (the second
+// rarely saves more than a LUT).
 // cut_leaves (3..6) bounds the cuts enumerated before support reduction:
 // wider finds smaller covers and costs more time.  On the 3000-gate random
 // DAGs of the benchmarks, three leaves take about 3 ms and six about 27 ms
 // for 4-6 % fewer LUTs.
-LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves);
+LutNet map_luts(const Circuit& c, const std::vector<uint32_t>& which, bool one_per_gate, int cut_leaves,
+                int recovery_passes = 2);
 
 // Gates in the cone of outputs `which`.
 uint32_t live_gate_count(const Circuit& c, const std::vector<uint32_t>& which);
