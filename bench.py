@@ -747,6 +747,8 @@ def run_serving(args, world, rank, local):
         srv_kw["max_slice_tiles"] = args.max_slice_tiles
     if args.tier_min_ms:
         srv_kw["tier_min_ms"] = args.tier_min_ms
+    if args.first_slice_tiles:
+        srv_kw["first_slice_tiles"] = args.first_slice_tiles
 
     peak_lop3, probe_mhz = ctx.lop3_peak()
     srv = api.Server(ctx, **srv_kw)
@@ -946,6 +948,7 @@ def main():
     ap.add_argument("--rollover", action="store_true", help="c4: servers with roll-over into the next slices")
     ap.add_argument("--max-slice-tiles", type=int, default=0, help="c4: largest slice of a job per epoch (tiles)")
     ap.add_argument("--tier-min-ms", type=int, default=0, help="c4: QSAT jobs estimated above this race a compiled kernel")
+    ap.add_argument("--first-slice-tiles", type=int, default=0, help="c4: a new job's first slice (tiles)")
     ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
