@@ -374,16 +374,18 @@ extern "C" int nsat_greedy_solve(nsat_ctx* ctx, nsat_circuit* c, const nsat_gree
                 r->wall_ms = now_ms() - t0;
                 return NSAT_OK;
             }
-            // write dest back to partition i of the image
+            // write dest back to partition i of the image; in device memory the
+            // next step's kernels follow in stream order, with no host wait
             if (w.storage == DEVICE) {
                 KCK(nsat_greedy_pack(w.dest, L, bits, w.dev_image + (uint64_t)i * pwords, sms, st));
             } else {
                 KCK(nsat_greedy_pack(w.dest, L, bits, w.stage[0], sms, st));
                 if (int rc = store(ctx, w, (uint64_t)i * pbytes, pbytes, w.stage[0], st, r)) return rc;
+                GCK(cudaStreamSynchronize(st));
             }
-            GCK(cudaStreamSynchronize(st));
         }
     }
+    GCK(cudaStreamSynchronize(st));   // the last write-back
     r->wall_ms = now_ms() - t0;
     return NSAT_OK;
 }
