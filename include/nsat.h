@@ -324,7 +324,7 @@ typedef struct {
     uint32_t max_active;        /* jobs sharing the device at once (<= 512); 0 = 512 */
     uint32_t max_queue;         /* waiting jobs before submit returns NSAT_EBUSY; 0 = 2^20 */
     uint32_t max_slice_tiles;   /* cap of one job's tiles per epoch; 0 = 4096 */
-    uint32_t first_slice_tiles; /* a new job's first slice (doubling after); 0 = 1 */
+    uint32_t first_slice_tiles; /* a new job's first slice (doubling after); 0 = 256 */
     uint64_t epoch_budget;      /* sum over jobs of tiles x program length per epoch; 0 = the
                                    budget nsat_server_tune persisted for this GPU, else 1.2e7
                                    (on a mixed serving trace: the most solves/s, the same p99

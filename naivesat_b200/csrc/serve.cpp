@@ -729,7 +729,12 @@ extern "C" int nsat_server_create(nsat_ctx* ctx, const nsat_server_opts* opts, n
     if (!s->opts.max_active || s->opts.max_active > kMaxActive) s->opts.max_active = kMaxActive;
     if (!s->opts.max_queue) s->opts.max_queue = 1u << 20;
     if (!s->opts.max_slice_tiles) s->opts.max_slice_tiles = 4096;
-    if (!s->opts.first_slice_tiles) s->opts.first_slice_tiles = 1;
+    // a new job starts with 256 tiles (2^23 assignments, well under a
+    // millisecond of interpreter time for the trace's circuits): on the mixed
+    // serving trace that measured 663 solves/s and p99 85 ms at 150/s, against
+    // 558-590 and 96-100 ms when every job started from one tile
+    if (!s->opts.first_slice_tiles) s->opts.first_slice_tiles = 256;
+    s->opts.first_slice_tiles = std::min(s->opts.first_slice_tiles, s->opts.max_slice_tiles);
     if (s->opts.shape > SRV_NSHAPES) return ctx_fail(ctx, NSAT_EINVAL, "no such interpreter shape");
     if (!s->opts.shape || !s->opts.epoch_budget) {
         // the tuned choice for this GPU, if one was persisted
