@@ -96,3 +96,23 @@ def test_no_stop_anywhere(ctx):
     rb.output(z)
     r = ctx.circuit(rb.fold()).stop_table().solve(n, mode=0)
     assert not r["found"] and r["rounds"] == 0
+
+
+def test_repeated_tables_reuse_the_context_pool(ctx):
+    """Tables come from the context's stream-ordered pool: building, solving
+    and freeing the same 2^24-state table many times gives the same answer
+    every time, and the device's free memory does not drift by more than
+    the pool keeps for reuse (8 GiB) plus one table pair."""
+    import torch
+    c = W.config("c3a")
+    h = ctx.circuit(c)
+    free0 = torch.cuda.mem_get_info(0)[0]
+    answers = set()
+    for _ in range(12):
+        t = h.stop_table()
+        r = t.solve(12, mode=1)
+        answers.add((r["found"], r.get("start"), r.get("end"), r["rounds"]))
+        t.close()
+    assert len(answers) == 1, answers
+    free1 = torch.cuda.mem_get_info(0)[0]
+    assert free0 - free1 <= (8 << 30) + 2 * (4 << 24), (free0, free1)
