@@ -63,7 +63,11 @@ typedef struct {
 } nsat_opts;
 
 /* ---- context ------------------------------------------------------------ */
-/* Replaces OpenCLBuilder::new(&device, config) / CPUBuilder::new (main.rs:278-300). */
+/* Replaces OpenCLBuilder::new(&device, config) / CPUBuilder::new (main.rs:278-300).
+ * A context owns a stream and a stream-ordered device memory pool for per-call
+ * buffers (SATOSTOP tables, partitioned images): freed buffers stay in the
+ * pool for the next call, up to 8 GiB; nsat_destroy returns them.  Tables are
+ * freed (nsat_table_free) before their context. */
 int nsat_create(int device, const nsat_opts* opts, nsat_ctx** out);
 void nsat_destroy(nsat_ctx* ctx);
 const char* nsat_strerror(int status);
