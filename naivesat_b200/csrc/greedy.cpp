@@ -147,9 +147,16 @@ int setup(nsat_ctx* ctx, Work& w, uint32_t n, uint64_t L, uint64_t chunk, const 
     } else {
         uint64_t budget = o->device_bytes;
         if (!budget) {
+            // free device memory less 1 GiB; if the image does not fit, what
+            // the context's pool keeps for reuse is returned and counted too
             size_t fr = 0, tot = 0;
             GCK(cudaMemGetInfo(&fr, &tot));
             budget = fr > (1ull << 30) ? fr - (1ull << 30) : 0;
+            if (w.bytes + work_dev > budget) {
+                ctx_trim(ctx);
+                GCK(cudaMemGetInfo(&fr, &tot));
+                budget = fr > (1ull << 30) ? fr - (1ull << 30) : 0;
+            }
         }
         w.storage = (w.bytes + work_dev <= budget) ? DEVICE : HOST;
     }

@@ -31,6 +31,9 @@ int ctx_fail(nsat_ctx* ctx, int code, const std::string& msg);
 // allocation.
 cudaError_t ctx_alloc(nsat_ctx* ctx, void** p, size_t bytes);
 void ctx_free(nsat_ctx* ctx, void* p);
+// Returns the pool's unused memory to the device (after the context's
+// stream finishes), for a caller about to size a buffer by free memory.
+void ctx_trim(nsat_ctx* ctx);
 
 // Circuit from the C ABI's flat description (not validated).
 Circuit circuit_from_desc(const nsat_circuit_desc* d);

@@ -956,6 +956,10 @@ cudaError_t nsat::ctx_alloc(nsat_ctx* ctx, void** p, size_t bytes) {
 void nsat::ctx_free(nsat_ctx* ctx, void* p) {
     if (p) cudaFreeAsync(p, ctx->stream);
 }
+void nsat::ctx_trim(nsat_ctx* ctx) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolTrimTo(ctx->pool, 0);
+}
 int nsat::ctx_sm_count(const nsat_ctx* ctx) { return ctx->sm_count; }
 bool nsat::ctx_no_optimize(const nsat_ctx* ctx) { return ctx->opts.no_optimize != 0; }
 nsat_opts nsat::ctx_opts(const nsat_ctx* ctx) { return ctx->opts; }
