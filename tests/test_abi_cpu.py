@@ -173,3 +173,12 @@ def test_lru_map_matches_model(tmp_path):
                     os.path.join(here, "lru_check.cpp"), "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+def test_short_search_cover_rule_is_for_solves_that_own_the_device():
+    """c0's 2^24 search is short next to cut mapping: a one-shot solve takes
+    one LUT per live gate (280), while the same circuit served (its device
+    time shared by every job) keeps the 170-LUT cut cover."""
+    c = W.config("c0")
+    assert api.jit_check(c, "sat")["lop3_ops"] == 280
+    assert api.server_program_check(c, "sat")[1] == 170
