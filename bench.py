@@ -664,6 +664,63 @@ def run_cold_probe(args):
 # --------------------------------------------------------------------------
 # config 4: batched serving
 
+def replay_probe(args, local, count, srv_kw, realtime=True, mode="replay", repeat=1):
+    """Runs one serving form over the first `count` requests of the trace in a
+    new process with empty kernel caches (this library's and the CUDA compute
+    cache).  Every request of the trace is a different circuit, so a server
+    in service compiles each QSAT tiering kernel once; replaying the same
+    requests in one process would find the kernels that an earlier replay
+    compiled.  mode "replay": the batched server (all requests at t=0, or at
+    their arrival times when realtime); mode "alone": one request at a time
+    through a server holding no other job.  With repeat=2 the same form runs
+    a second time in the same process (every kernel cached).  Returns the
+    child's JSON: per run the verdicts, compiled blocks, latencies, makespan
+    and server counters."""
+    tmp = tempfile.mkdtemp(prefix="nsat_replay_")
+    env = dict(os.environ, NSAT_JIT_CACHE=tmp, CUDA_CACHE_PATH=os.path.join(tmp, "cuda"))
+    spec = {"count": count, "realtime": realtime, "srv_kw": srv_kw, "mode": mode, "repeat": repeat,
+            "requests": args.requests, "rate": args.rate}
+    cmd = [sys.executable, os.path.abspath(__file__), "--replay-probe", json.dumps(spec), "--device", str(local)]
+    try:
+        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=1800)
+        for line in out.stdout.splitlines()[::-1]:
+            if line.startswith("{"):
+                return json.loads(line)
+        raise RuntimeError("replay probe printed no result: " + out.stderr[-2000:])
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def run_replay_probe(args):
+    from naivesat_b200 import api, serving, workloads as W
+    spec = json.loads(args.replay_probe)
+    ctx = api.Context(args.device)
+    reqs = W.serving_requests(spec["requests"], seed=2024, rate_hz=spec["rate"])[:spec["count"]]
+    warm = W.serving_requests(64, seed=99, rate_hz=1e9)
+    kw = spec["srv_kw"]
+    srv = api.Server(ctx, **kw)
+    serving.replay_server(srv, warm, realtime=False)      # graphs captured, context warm
+    srv.close()
+    runs = []
+    for _ in range(spec["repeat"]):
+        srv = api.Server(ctx, **kw)
+        if spec["mode"] == "alone":
+            res, service = serving.interpreter_alone_service_times(srv, reqs)
+            lat, mk = service, sum(service)
+        else:
+            res, lat, mk = serving.replay_server(srv, reqs, realtime=spec["realtime"])
+        st = srv.stats()
+        srv.close()
+        keys = sorted(res)
+        runs.append({"verdicts": [list(serving.verdict(reqs[k]["kind"], res[k])) for k in keys],
+                     "compiled_blocks": [res[k]["compiled_blocks"] for k in keys],
+                     "tiles": [res[k]["tiles"] for k in keys],
+                     "lat": lat, "makespan": mk, "epochs": st["epochs"], "device_ms": st["device_ms"],
+                     "shape": st["shape"]})
+    print(json.dumps({"runs": runs}), flush=True)
+    ctx.close()
+
+
 def serving_cpu_baseline(reqs, threads, target_s):
     """The oracle port solving requests in order on the host cores for about
     target_s seconds; returns (solves/s, sample description)."""
@@ -750,11 +807,18 @@ def run_serving(args, world, rank, local):
     if args.first_slice_tiles:
         srv_kw["first_slice_tiles"] = args.first_slice_tiles
 
+    # every server of this run (here and in the fresh processes below) with the
+    # same explicit shape and budget
+    srv_kw.setdefault("shape", tune["shape"])
+    srv_kw.setdefault("epoch_budget", tune.get("epoch_budget") or 12000000)
+
     peak_lop3, probe_mhz = ctx.lop3_peak()
     srv = api.Server(ctx, **srv_kw)
     serving.replay_server(srv, warm, realtime=False)      # graphs captured, context warm
     srv.close()
 
+    # the saturated run: the first replay of the trace in this process, so its
+    # QSAT tiering compiles every kernel it uses
     clocks = ClockSampler(local)
     clocks.start()
     srv = api.Server(ctx, **srv_kw)
@@ -762,66 +826,49 @@ def run_serving(args, world, rank, local):
     st_sat = srv.stats()
     srv.close()
     clk = clocks.stop()
-    srv = api.Server(ctx, **srv_kw)
-    res_poi, lat_poi, mk_poi = serving.replay_server(srv, reqs, realtime=True)
-    st_poi = srv.stats()
-    srv.close()
+    # the Poisson run in a new process with empty kernel caches: a replay here
+    # would find the tiering kernels the saturated run compiled
+    poi = replay_probe(args, local, len(reqs), srv_kw, realtime=True)["runs"][0]
+    lat_poi, mk_poi = poi["lat"], poi["makespan"]
+    st_poi = {"epochs": poi["epochs"]}
     for i in res_sat:
-        assert serving.verdict(reqs[i]["kind"], res_sat[i]) == serving.verdict(reqs[i]["kind"], res_poi[i]), i
+        assert tuple(poi["verdicts"][i]) == serving.verdict(reqs[i]["kind"], res_sat[i]), i
 
     # the plain forms, one request at a time, on the first kp requests of the
     # trace (kp: what the compile-bound form gets through in plain_seconds):
     # compiled one-shot solvers with an empty kernel cache (a new process per
-    # circuit), the same with every kernel already in the on-disk cache, and
-    # the precompiled interpreter serving one job at a time (no batching)
+    # circuit) and the same with every kernel already in the on-disk cache; the
+    # precompiled interpreter serving one job at a time (no batching) and the
+    # batched server on the same requests, each in a new process with empty
+    # kernel caches, and the server once more with its kernels cached
     cache_dir = tempfile.mkdtemp(prefix="nsat_plain_")
     try:
         pres, service = serving.plain_service_times(ctx, reqs, args.plain_seconds, cache_dir=cache_dir)
         kp = len(service)
         prefix = reqs[:kp]
         wres, wservice = serving.plain_service_times(ctx, prefix, 1e9, cache_dir=cache_dir)
-        # the server with the same warm kernel cache (its QSAT tiering finds
-        # the kernels compiled): the like-for-like partner of the warm form
-        old_cache = os.environ.get("NSAT_JIT_CACHE")
-        os.environ["NSAT_JIT_CACHE"] = cache_dir
-        try:
-            srv = api.Server(ctx, **srv_kw)
-            wbres, wblat, wbmk = serving.replay_server(srv, prefix, realtime=False)
-            srv.close()
-            srv = api.Server(ctx, **srv_kw)
-            wpres, wplat, wpmk = serving.replay_server(srv, prefix, realtime=True)
-            srv.close()
-        finally:
-            if old_cache is None:
-                os.environ.pop("NSAT_JIT_CACHE", None)
-            else:
-                os.environ["NSAT_JIT_CACHE"] = old_cache
     finally:
         shutil.rmtree(cache_dir, ignore_errors=True)
-    srv = api.Server(ctx, **srv_kw)
-    ires, iservice = serving.interpreter_alone_service_times(srv, prefix)
-    srv.close()
-    # the batched server on the same requests: all queued at t=0, and Poisson
-    srv = api.Server(ctx, **srv_kw)
-    bres, blat, bmk = serving.replay_server(srv, prefix, realtime=False)
-    srv.close()
-    srv = api.Server(ctx, **srv_kw)
-    pres_b, plat_b, pmk_b = serving.replay_server(srv, prefix, realtime=True)
-    srv.close()
+    alone = replay_probe(args, local, kp, srv_kw, mode="alone")["runs"][0]
+    iservice = alone["lat"]
+    bsat = replay_probe(args, local, kp, srv_kw, realtime=False, repeat=2)["runs"]
+    bpoi = replay_probe(args, local, kp, srv_kw, realtime=True, repeat=2)["runs"]
     same = 0
     for i in range(kp):
         v = serving.verdict(reqs[i]["kind"], res_sat[i])
-        forms = (pres[i], wres[i], ires[i], bres[i], pres_b[i], wbres[i], wpres[i])
-        assert all(serving.verdict(reqs[i]["kind"], f) == v for f in forms), i
+        forms = [serving.verdict(reqs[i]["kind"], f) for f in (pres[i], wres[i])] + \
+                [tuple(r["verdicts"][i]) for r in [alone] + bsat + bpoi]
+        assert all(f == v for f in forms), i
         same += 1
     arr = [r["arrival_s"] for r in prefix]
-    server_prefix = serving.summarize(plat_b, pmk_b, kp)
-    server_prefix["solves_per_s"] = kp / bmk
-    server_prefix["note"] = "solves/s with the requests queued at t=0; latencies under the Poisson arrivals"
-    server_warm = serving.summarize(wplat, wpmk, kp)
-    server_warm["solves_per_s"] = kp / wbmk
-    server_warm["note"] = ("the same with the warm kernel cache of the compiled_warm_cache form (QSAT tiering "
-                           "loads its kernels instead of compiling them)")
+    server_prefix = serving.summarize(bpoi[0]["lat"], bpoi[0]["makespan"], kp)
+    server_prefix["solves_per_s"] = kp / bsat[0]["makespan"]
+    server_prefix["note"] = ("a new process with empty kernel caches: solves/s with the requests queued at t=0, "
+                             "latencies under the Poisson arrivals")
+    server_warm = serving.summarize(bpoi[1]["lat"], bpoi[1]["makespan"], kp)
+    server_warm["solves_per_s"] = kp / bsat[1]["makespan"]
+    server_warm["note"] = ("the same server replaying the requests a second time in that process, every QSAT "
+                           "tiering kernel cached: the like-for-like partner of the warm compiled form")
 
     def one_at_a_time(svc, form):
         lat = serving.fifo_latencies(arr, svc)
@@ -837,7 +884,8 @@ def run_serving(args, world, rank, local):
     plain_forms = {
         "requests": kp, "rate_hz": args.rate, "server": server_prefix, "server_warm_cache": server_warm,
         "interpreter_alone": one_at_a_time(iservice, "the precompiled interpreter, one job per server at a "
-                                                     "time (same server options, no batching)"),
+                                                     "time (same server options, no batching), in a new "
+                                                     "process with empty kernel caches"),
         "compiled_warm_cache": one_at_a_time(wservice, "one-shot solvers with every kernel already in the "
                                                        "on-disk cache (a second pass over the same requests)"),
         "compiled_cold_cache": one_at_a_time(service, "one-shot solvers with an empty kernel cache (per-circuit "
@@ -874,14 +922,14 @@ def run_serving(args, world, rank, local):
         cpu = {"value": v, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample + ", " + cpu_model()}
     kinds = {k: sum(1 for r in reqs if r["kind"] == k) for k in ("sat", "qsat", "stop")}
     sat_sum = serving.summarize(lat_sat, mk_sat, len(res_sat))
-    poi_sum = serving.summarize(lat_poi, mk_poi, len(res_poi))
+    poi_sum = serving.summarize(lat_poi, mk_poi, len(lat_poi))
+    poi_sum["note"] = "a new process with empty kernel caches (QSAT tiering compiles its kernels during the run)"
     # where the tail comes from: percentiles per kind, and for the QSAT jobs
     # that raced a compiled kernel
-    keys = sorted(res_poi)
     groups = {}
-    for k, lat in zip(keys, lat_poi):
+    for k, lat in enumerate(lat_poi):
         groups.setdefault(reqs[k]["kind"], []).append(lat)
-        if res_poi[k]["compiled_blocks"]:
+        if poi["compiled_blocks"][k]:
             groups.setdefault("qsat_tiered", []).append(lat)
     poi_sum["by_kind"] = {g: {"requests": len(v), "p50_ms": serving.percentile(v, 50) * 1e3,
                               "p99_ms": serving.percentile(v, 99) * 1e3} for g, v in groups.items()}
@@ -950,10 +998,14 @@ def main():
     ap.add_argument("--tier-min-ms", type=int, default=0, help="c4: QSAT jobs estimated above this race a compiled kernel")
     ap.add_argument("--first-slice-tiles", type=int, default=0, help="c4: a new job's first slice (tiles)")
     ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--replay-probe", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.cold_probe:
         run_cold_probe(args)
+        return
+    if args.replay_probe:
+        run_replay_probe(args)
         return
     # NVRTC keeps compiled kernels in the CUDA compute cache (CUDA_CACHE_PATH,
     # by default shared by every process of the user), so a kernel that an
