@@ -806,6 +806,8 @@ def run_serving(args, world, rank, local):
         srv_kw["tier_min_ms"] = args.tier_min_ms
     if args.first_slice_tiles:
         srv_kw["first_slice_tiles"] = args.first_slice_tiles
+    if args.tier_threads:
+        srv_kw["tier_threads"] = args.tier_threads
 
     # every server of this run (here and in the fresh processes below) with the
     # same explicit shape and budget
@@ -997,6 +999,7 @@ def main():
     ap.add_argument("--max-slice-tiles", type=int, default=0, help="c4: largest slice of a job per epoch (tiles)")
     ap.add_argument("--tier-min-ms", type=int, default=0, help="c4: QSAT jobs estimated above this race a compiled kernel")
     ap.add_argument("--first-slice-tiles", type=int, default=0, help="c4: a new job's first slice (tiles)")
+    ap.add_argument("--tier-threads", type=int, default=0, help="c4: QSAT tiering workers")
     ap.add_argument("--cold-probe", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--replay-probe", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--device", type=int, default=0, help=argparse.SUPPRESS)
