@@ -240,12 +240,37 @@ class QsatWorkload:
                 "lop3_per_word": self.lop3, "live_gates": self.live}
 
     def cpu(self, threads, target_s=12.0):
-        from oracle import oracle as O
+        """The reference's CPU QSAT path restated as generated C (oracle/
+        cpu_codegen.py: per-circuit vector code in v-order, calls reduced to
+        their first-block units, the first block's QuantReducer), full solves
+        repeated for about target_s / 3; beside it the oracle's interpreter
+        (one QuantReducer push per item) for the factor between the two.
+        The two FinalResults must agree."""
+        from oracle import cpu_codegen as CG, oracle as O
         oc = O.Circuit(self.circ.n, self.circ.gates, self.circ.outputs)
+        work = (1 << self.circ.n) * self.circ.num_gates
         t0 = time.perf_counter()
-        O.qsat(oc, self.circ.quants, mode=1, threads=threads)
-        dt = time.perf_counter() - t0
-        return (1 << self.circ.n) * self.circ.num_gates / dt, "full oracle solve (%.1f s)" % dt
+        ref = O.qsat(oc, self.circ.quants, mode=1, threads=threads)
+        dti = time.perf_counter() - t0
+        irate = work / dti
+        try:
+            g = CG.CodegenQsat(self.circ, self.circ.quants)
+        except ValueError:      # units smaller than a vector word: the interpreter only
+            return irate, "full oracle solve (%.1f s)" % dti
+        reps, dt = 0, 0.0
+        while reps < 1 or (dt < target_s / 3 and reps < 200):
+            t0 = time.perf_counter()
+            got = g.solve(threads)
+            dt += time.perf_counter() - t0
+            reps += 1
+        g.close()
+        assert got == ref, (got, ref)
+        rate = reps * work / dt
+        return rate, ("generated C per circuit, %d-bit vectors, gcc -O3 -march=native, OpenMP over args of 2^%d "
+                      "items, first-block QuantReducer over the calls' units; %d full solve(s) in %.2f s"
+                      % (g.vector_bits, g.e, reps, dt)), \
+            {"method": "codegen", "interpreter_value": irate,
+             "interpreter_sample": "full oracle solve (%.1f s)" % dti, "codegen_over_interpreter": rate / irate}
 
 
 def gather_roofline(ctx, log2_table, gathers, stream_bytes, ms, hbm_gbs):
@@ -467,9 +492,9 @@ def run_reference(args, world, rank):
     wl = make_workload(args.workload, args.log2)
     threads = os.cpu_count() or 1
     if wl.kind != "sat":
-        vals = [wl.cpu(threads)[0] for _ in range(max(1, args.steps))]
-        rate = statistics.median(vals)
-        sample = "full oracle solve per step"
+        outs = [wl.cpu(threads) for _ in range(max(1, args.steps))]
+        rate = statistics.median(o[0] for o in outs)
+        sample = outs[-1][1] + " per step"
         span = None
     else:
         # the reference's CPU path restated as generated C per circuit

@@ -370,9 +370,15 @@ int or_qr_push(or_qr* qr, uint64_t index, int item) {
 /* the items of packed words (item k = bit k%32 of word k/32), in index order,
  * until the reducer is final; test helper for the device reduction */
 int or_qr_push_words(or_qr* qr, const uint32_t* words, uint64_t nwords) {
+    return or_qr_push_words_from(qr, 0, words, nwords);
+}
+
+/* Items first .. first + 32 nwords - 1: item first + k is bit k % 32 of
+ * word k / 32 (consecutive batches of one item sequence). */
+int or_qr_push_words_from(or_qr* qr, uint64_t first, const uint32_t* words, uint64_t nwords) {
     for (uint64_t k = 0; k < nwords * 32u; k++) {
         if (qr_is_end(qr) || qr->has_solution) break;
-        if (or_qr_push(qr, k, (int)((words[k >> 5] >> (k & 31u)) & 1u))) return -1;
+        if (or_qr_push(qr, first + k, (int)((words[k >> 5] >> (k & 31u)) & 1u))) return -1;
     }
     return 0;
 }

@@ -54,6 +54,7 @@ void or_qr_free(or_qr* qr);
 int or_qr_push(or_qr* qr, uint64_t index, int item);
 /* pushes item k = bit k%32 of words[k/32] for k = 0.. in order, until final */
 int or_qr_push_words(or_qr* qr, const uint32_t* words, uint64_t nwords);
+int or_qr_push_words_from(or_qr* qr, uint64_t first, const uint32_t* words, uint64_t nwords);
 /* returns 1 and fills the FinalResult fields when final, else 0 */
 int or_qr_final(const or_qr* qr, int* reversed, uint32_t* solution_bits,
                 int* has_solution, uint64_t* solution);

@@ -48,6 +48,7 @@ def lib():
             L.or_qr_free.argtypes = [C.c_void_p]
             L.or_qr_push.argtypes = [C.c_void_p, C.c_uint64, C.c_int]
             L.or_qr_push_words.argtypes = [C.c_void_p, U32P, C.c_uint64]
+            L.or_qr_push_words_from.argtypes = [C.c_void_p, C.c_uint64, U32P, C.c_uint64]
             L.or_qr_final.argtypes = [C.c_void_p, C.POINTER(C.c_int), U32P, C.POINTER(C.c_int), U64P]
             L.or_qsat.argtypes = [C.POINTER(OrCircuit), U8P, C.c_int, C.c_int, C.POINTER(C.c_int),
                                   U32P, C.POINTER(C.c_int), U64P]
@@ -128,11 +129,11 @@ class QuantReducer:
     def push(self, index, item):
         assert lib().or_qr_push(self._h, index, int(bool(item))) == 0
 
-    def push_words(self, words):
-        """Items of packed 32-bit words (item k = bit k%32 of word k/32), in
-        index order from 0."""
+    def push_words(self, words, first=0):
+        """Items of packed 32-bit words (item first + k = bit k%32 of word
+        k/32), in index order from `first`."""
         w = np.ascontiguousarray(np.asarray(words, dtype=np.uint32))
-        assert lib().or_qr_push_words(self._h, _ptr(w, U32P), len(w)) == 0
+        assert lib().or_qr_push_words_from(self._h, first, _ptr(w, U32P), len(w)) == 0
 
     def final_result(self):
         rv, sb, hs, sol = C.c_int(), C.c_uint32(), C.c_int(), C.c_uint64()
